@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the direct-SCF J/K build on B200.
+
+Workload (default): (H2O)_96, rigid waters in a 15 A cube (seed 20261204),
+6-31G* shell structure (synthetic exponents, see
+electrolites_b200/basis_synth.py), Cartesian AOs, UHF density pair
+D_alpha = D_atom/2, D_beta = D_alpha + symmetric Gaussian noise
+(sigma = 1e-3 max|D_alpha|), hermi = 1, J and K, direct_scf_tol 1e-13,
+plain all-FP64 form.  One step = one J/K build of both densities.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--mixed THRESHOLD]
+
+Prints one JSON line (rank 0).  value = J/K builds per second of the whole
+job (device-timed with CUDA events, densities resident in HBM); e2e = the
+same through jk_build_host from pinned host buffers, copies included.  With
+N > 1 every rank runs its own build of the same workload (replicas, weak
+scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (waters, cube edge A, basis, UHF pair, seed)
+    'h2o96_631gs_uhf': (96, 15.0, '6-31g*', True, 20261204),
+    'h2o8_631gs': (8, 7.0, '6-31g*', False, 20261203),
+    'h2o64_tzvp': (64, 12.5, 'def2-tzvp', False, 20261205),
+}
+DEFAULT = 'h2o96_631gs_uhf'
+TOL = 1e-13
+L2_FLUSH_BYTES = 256 << 20      # > 126 MB L2
+
+
+def make_inputs(name):
+    import numpy as np
+    from electrolites_b200 import clusters
+    n, edge, basis, uhf, seed = WORKLOADS[name]
+    mol = clusters.water_mole(n, edge, seed, basis=basis, cart=True)
+    D = clusters.atomic_density(mol, seed)
+    dms = clusters.uhf_pair(D, seed + 1) if uhf else D[None]
+    return mol, np.ascontiguousarray(dms)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix='.csv')
+            os.close(fd)
+            self.f = open(self.path, 'w')
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
+                 '-lms', '200', '-i', str(self.device)], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = [r.split(',') for r in open(self.path).read().strip().splitlines() if r]
+        os.unlink(self.path)
+        sm, smax, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = max(smax, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if 'Active' in v and 'Not' not in v:
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': smax,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_sample(mol, dms, budget_s=15.0, nthreads=0, seed=1):
+    """Oracle J/K on a random sample of bra shell pairs, scaled to a full
+    build: returns (builds/s, threads, description)."""
+    import numpy as np
+    from oracle import oracle as O
+    nthreads = nthreads or os.cpu_count() or 1
+    npair = mol.nbas * (mol.nbas + 1) // 2
+    rng = np.random.default_rng(seed)
+    n, spent, nq_tot, used = 8, 0.0, 0, 0
+    while spent < budget_s and used < npair:
+        take = rng.choice(npair, size=min(n, npair - used), replace=False)
+        t0 = time.perf_counter()
+        _, _, nq = O.jk_sample(mol, dms, take, tol=TOL, nthreads=nthreads)
+        spent += time.perf_counter() - t0
+        used += len(take)
+        nq_tot += nq
+        n = max(8, int(n * min(4.0, max(1.5, budget_s / max(spent, 1e-3) / 2))))
+    t_full = spent * npair / used
+    desc = (f'{used} of {npair} bra shell pairs drawn uniformly (seed {seed}), all '
+            f'their kets, {nq_tot} quartets in {spent:.1f} s; time scaled by '
+            f'{npair / used:.1f} to a full build')
+    return 1.0 / t_full, nthreads, desc
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    mol, dms = make_inputs(args.workload)
+    vals = []
+    threads, desc = os.cpu_count(), ''
+    for it in range(args.warmup + args.steps):
+        v, threads, desc = cpu_sample(mol, dms, budget_s=min(20.0, 60.0 / max(1, args.steps)),
+                                      seed=1 + it)
+        if it >= args.warmup:
+            vals.append(v)
+    v = statistics.mean(vals)
+    line = {'impl': 'reference', 'metric': 'jk_builds_per_s', 'value': v,
+            'unit': 'builds/s', 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 / v, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': args.workload, 'hermi': 1, 'direct_scf_tol': TOL,
+                       'form': 'plain'},
+            'cpu_baseline': {'value': v, 'unit': 'builds/s', 'cores': threads,
+                             'kind': 'port', 'sample': desc},
+            'e2e': {'value': v, 'unit': 'builds/s', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from electrolites_b200 import _lib, flop_model
+    from electrolites_b200.jk import VHFOpt
+
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    mol, dms_h = make_inputs(args.workload)
+    n_dm = dms_h.shape[0]
+    opt = VHFOpt(mol, TOL, device=local).build()
+    opt.set_timing(True)
+    dms = torch.as_tensor(dms_h, device=dev)
+    vj = torch.empty_like(dms)
+    vk = torch.empty_like(dms)
+    flush = torch.empty(L2_FLUSH_BYTES // 8, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    thr = float(args.mixed)
+
+    def one():
+        opt.build_jk_async(dms, 1, True, True, vj, vk, thr, stream)
+
+    for _ in range(max(3, args.warmup)):
+        one()
+    opt.sync(stream)
+
+    peak = ctypes.c_double()
+    _lib.check(_lib.lib().jk_fp64_peak(local, ctypes.byref(peak)), 'jk_fp64_peak')
+    peak_tflops = peak.value
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = []
+    class_ms = {}
+    launches = 0
+    for _ in range(args.steps):
+        flush.zero_()                                   # L2 flush, outside the timing
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        one()
+        e.record(stream)
+        evs.append((s, e))
+        cm, launches = opt.last_class_ms()             # syncs; between steps
+        for k, v in cm.items():
+            class_ms[k] = class_ms.get(k, 0.0) + v
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    opt.sync(stream)
+    step_ms = [s.elapsed_time(e) for s, e in evs]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+
+    # algorithmic flops of one build
+    stats = opt.class_counts()
+    n_k, n_j = n_dm, n_dm
+    flops = flop_model.build_flops(stats, n_j, n_k)
+    for k in class_ms:
+        class_ms[k] /= args.steps
+    dom = max(class_ms, key=class_ms.get) if class_ms else None
+    dom_flops = flop_model.build_flops({dom: stats[dom]}, n_j, n_k) if dom else 0
+    achieved = dom_flops / (class_ms[dom] * 1e-3) / 1e12 if dom else 0.0
+
+    # e2e through the host-buffer entry point, pinned buffers
+    dm_pin = torch.as_tensor(dms_h).pin_memory()
+    vj_pin = torch.empty_like(dm_pin).pin_memory()
+    vk_pin = torch.empty_like(dm_pin).pin_memory()
+    L = _lib.lib()
+
+    def one_host():
+        _lib.check(L.jk_build_host(opt.plan, ctypes.c_void_p(dm_pin.data_ptr()), n_dm, 1, 1, 1,
+                                   ctypes.c_void_p(vj_pin.data_ptr()),
+                                   ctypes.c_void_p(vk_pin.data_ptr()), thr,
+                                   ctypes.c_void_p(stream.cuda_stream)), 'jk_build_host')
+    one_host()
+    e2e_steps = max(1, min(args.steps, 3))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        one_host()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    bytes_in = dm_pin.numel() * 8
+    bytes_out = 2 * dm_pin.numel() * 8
+
+    # correctness guard on the timed output: symmetric, finite
+    assert torch.isfinite(vj).all() and torch.isfinite(vk).all()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, thr_used, desc = cpu_sample(mol, dms_h, budget_s=args.cpu_budget)
+        cpu = {'value': v, 'unit': 'builds/s', 'cores': thr_used, 'kind': 'port',
+               'sample': desc}
+
+    if rank == 0:
+        nq = sum(v[0] for v in stats.values())
+        line = {
+            'metric': 'jk_builds_per_s', 'value': world * 1e3 / ms_per_step, 'unit': 'builds/s',
+            'n_gpus': world, 'steps': args.steps, 'warmup': max(3, args.warmup),
+            'ms_per_step': ms_per_step, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64' if thr <= 0 else 'f64+f32',
+            'data': 'synthetic',
+            'config': {'workload': args.workload, 'nao_cart': mol.nao_cart, 'nbas': mol.nbas,
+                       'n_dm': n_dm, 'hermi': 1, 'direct_scf_tol': TOL,
+                       'form': 'plain' if thr <= 0 else f'mixed {thr:g}',
+                       'parallelism': f'replicas{world}',
+                       'l2': 'flushed between steps (256 MB write, untimed)',
+                       'quartets': nq, 'build_tflops': flops / (ms_per_step * 1e-3) / 1e12,
+                       'fp64_peak_tflops': peak_tflops,
+                       'fp64_peak_frac': flops / (ms_per_step * 1e-3) / 1e12 / peak_tflops,
+                       'class_ms': {''.join(map(str, k)): round(v, 3) for k, v in
+                                    sorted(class_ms.items(), key=lambda kv: -kv[1])[:12]}},
+            'roofline': {'bound': 'fp64', 'kernel': 'jk_class_kernel ' + ''.join(map(str, dom)) if dom else None,
+                         'achieved': achieved, 'peak': peak_tflops, 'unit': 'TFLOP/s',
+                         'frac': achieved / peak_tflops if peak_tflops else None,
+                         'peak_source': 'in-run FP64 FMA probe (jk_fp64_peak)',
+                         'traffic': None},
+            'e2e': {'value': world / e2e_s, 'unit': 'builds/s', 'h2d_bytes_per_step': bytes_in,
+                    'd2h_bytes_per_step': bytes_out},
+            'gpu_launches': launches * args.steps,
+            'clocks': clk,
+            'cpu_baseline': cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument('--mixed', type=float, default=0.0)
+    ap.add_argument('--cpu-budget', type=float, default=15.0)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    rank = int(os.environ.get('RANK', 0))
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,123 @@
+"""B200-native direct-SCF Coulomb/exchange (J/K) engine.
+
+Public API:
+  * ``jk.VHFOpt`` -- a plan per molecule (device-resident pair and screening
+    tables), with ``get_jk`` / ``get_k`` / ``get_j``;
+  * ``jk.get_jk(mol, dm, ...)``, ``jk.get_j``, ``jk.get_k`` -- GPU4PySCF's
+    module-level signatures;
+  * ``patch(*names)`` / ``patch_all()`` -- install the engine in place of
+    GPU4PySCF's ``_VHFOpt.get_jk`` / ``get_k`` and ``j_engine._VHFOpt.get_j``,
+    the targets the reference patches (electrolites/__init__.py:59-61, 107,
+    329-350).  ``check_targets()`` reports which targets exist.
+"""
+from __future__ import annotations
+
+import importlib
+
+from . import jk  # noqa: F401
+
+__all__ = ['jk', 'patch', 'patch_all', 'patched', 'check_targets', 'MODULES']
+
+# name -> (module path, class name, method name)
+_TARGETS = {
+    'fastjk': ('gpu4pyscf.scf.jk', '_VHFOpt', 'get_jk'),
+    'fastk': ('gpu4pyscf.scf.jk', '_VHFOpt', 'get_k'),
+    'fastj': ('gpu4pyscf.scf.j_engine', '_VHFOpt', 'get_j'),
+}
+MODULES = tuple(_TARGETS)
+_PATCHED = {}
+
+
+def check_targets():
+    """{name: None if the target exists, else the reason it does not}."""
+    out = {}
+    for name, (mod, cls, meth) in _TARGETS.items():
+        try:
+            m = importlib.import_module(mod)
+            c = getattr(m, cls)
+            getattr(c, meth)
+            out[name] = None
+        except Exception as err:   # noqa: BLE001
+            out[name] = f'{type(err).__name__}: {err}'
+    return out
+
+
+def _plan_for(opt):
+    """The engine plan attached to a GPU4PySCF option object, built from its
+    sorted Cartesian molecule on first use."""
+    plan = getattr(opt, '_jk_b200', None)
+    if plan is None:
+        mol = getattr(opt, 'sorted_mol', None) or opt.mol
+        tol = getattr(opt, 'direct_scf_tol', jk.DEFAULT_TOL)
+        plan = jk.VHFOpt(_CartView(mol), tol).build()
+        opt._jk_b200 = plan
+    return plan
+
+
+class _CartView:
+    """A molecule seen through its Cartesian AO layout (GPU4PySCF's option
+    objects work in the sorted Cartesian basis)."""
+
+    def __init__(self, mol):
+        self._m = mol
+        self._atm, self._bas, self._env = mol._atm, mol._bas, mol._env
+
+    def ao_loc_nr(self, cart=True):
+        return self._m.ao_loc_nr(cart=True)
+
+
+def _out(x, like):
+    if hasattr(like, '__cuda_array_interface__') and not hasattr(like, 'data_ptr'):
+        import cupy
+        return cupy.asarray(x)
+    return x
+
+
+def _get_jk(self, dms, hermi, verbose=None):
+    if callable(dms):
+        dms = dms()
+    vj, vk = _plan_for(self).get_jk(dms, hermi, verbose)
+    return _out(vj, dms), _out(vk, dms)
+
+
+def _get_k(self, dms, hermi, verbose=None, omega=None, lr_factor=None, sr_factor=None):
+    if callable(dms):
+        dms = dms()
+    return _out(_plan_for(self).get_k(dms, hermi, verbose, omega, lr_factor, sr_factor), dms)
+
+
+def _get_j(self, dms, verbose=None):
+    if callable(dms):
+        dms = dms()
+    return _out(_plan_for(self).get_j(dms, verbose), dms)
+
+
+_IMPL = {'fastjk': _get_jk, 'fastk': _get_k, 'fastj': _get_j}
+
+
+def patch(*names):
+    """Install the engine for the named targets ('fastjk', 'fastk',
+    'fastj').  Raises if a target does not exist (no silent partial
+    patching)."""
+    status = check_targets()
+    for name in names:
+        if name not in _TARGETS:
+            raise KeyError(f'unknown target {name!r}; known: {MODULES}')
+        if status[name] is not None:
+            raise ImportError(f'cannot patch {name}: {status[name]}')
+    for name in names:
+        if name in _PATCHED:
+            continue
+        mod, cls, meth = _TARGETS[name]
+        c = getattr(importlib.import_module(mod), cls)
+        _PATCHED[name] = getattr(c, meth)
+        setattr(c, meth, _IMPL[name])
+    return list(_PATCHED)
+
+
+def patch_all():
+    return patch(*MODULES)
+
+
+def patched():
+    return sorted(_PATCHED)

@@ -1,0 +1,388 @@
+"""Code generator for the per-angular-momentum-class ERI + J/K kernels.
+
+For every quartet class (li lj | lk ll) with li >= lj, lk >= ll and the bra
+pair class >= the ket pair class (55 classes up to f), this writes one CUDA
+translation unit under csrc/generated/ holding
+
+  * a `Cls_<li><lj><lk><ll>` struct of straight-line device functions:
+      - `root_acc`: one Rys root's 2D integrals G_d[e][f] (VRR on centres i
+        and k, e <= li+lj, f <= lk+ll) and the accumulation of the
+        (e0|f0) Cartesian integrals, all in registers (register form);
+      - `row_acc`: the accumulation for one runtime e-component given its
+        three rows of 2D integrals (team form, rows staged in shared memory);
+      - `hrr_bra` / `hrr_ket`: the horizontal transfers (e0| -> (ij| and
+        |f0) -> |kl), applied once per contracted quartet;
+  * the instantiation of the kernel template of csrc/jk_kernels.cuh for
+    that class, and a host launcher registered in a table.
+
+The arithmetic follows the reference's Rys formulation (roots t^2, c0x, cpx,
+b00, b10, b01 recurrences: electrolites/codegen/gen_khigh.py:128-181) with
+one structural change: the transfer to the j and l centres is applied after
+the primitive and root sums (late HRR) instead of per root and primitive.
+
+Form selection: the register form is used when the (e0|f0) block has at most
+REG_MAX elements; otherwise the team form spreads the e-components over the
+lanes of a team (16 or 32*k threads) and splits the f-components over warps.
+"""
+from __future__ import annotations
+
+import os
+import sys
+from dataclasses import dataclass
+
+REG_MAX = 81          # largest (e0|f0) block kept in one thread's registers
+FPART_MAX = 40        # f-components per warp in the team form
+LMAX = 3
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def comps(l):
+    return [(lx, ly, l - lx - ly) for lx in range(l, -1, -1)
+            for ly in range(l - lx, -1, -1)]
+
+
+def cidx(l, c):
+    lx, ly, lz = c
+    return (l - lx) * (l - lx + 1) // 2 + lz
+
+
+@dataclass
+class Cls:
+    li: int
+    lj: int
+    lk: int
+    ll: int
+
+    @property
+    def tag(self):
+        return f'{self.li}{self.lj}{self.lk}{self.ll}'
+
+    @property
+    def lij(self):
+        return self.li + self.lj
+
+    @property
+    def lkl(self):
+        return self.lk + self.ll
+
+    @property
+    def nroots(self):
+        return (self.lij + self.lkl) // 2 + 1
+
+    def eset(self):
+        return [(L, c) for L in range(self.li, self.lij + 1) for c in comps(L)]
+
+    def fset(self):
+        return [(L, c) for L in range(self.lk, self.lkl + 1) for c in comps(L)]
+
+    @property
+    def ne(self):
+        return len(self.eset())
+
+    @property
+    def nf(self):
+        return len(self.fset())
+
+    @property
+    def form(self):
+        return 'reg' if self.ne * self.nf <= REG_MAX else 'team'
+
+    # team form geometry
+    @property
+    def team_lanes(self):          # lanes holding e-components
+        return 16 if self.ne <= 16 else 32 * ((self.ne + 31) // 32)
+
+    @property
+    def nwf(self):                 # warps (or half-warp teams) over f
+        return (self.nf + FPART_MAX - 1) // FPART_MAX
+
+    @property
+    def team_threads(self):
+        return self.team_lanes * self.nwf
+
+    def fparts(self):
+        n = self.nwf
+        size = (self.nf + n - 1) // n
+        return [(p * size, min(self.nf, (p + 1) * size)) for p in range(n)]
+
+
+def all_classes(lmax=LMAX):
+    pairs = [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
+    out = []
+    for A in range(len(pairs)):
+        for B in range(A + 1):
+            li, lj = pairs[A]
+            lk, ll = pairs[B]
+            out.append((A, B, Cls(li, lj, lk, ll)))
+    return out
+
+
+def pair_class_index(la, lb):
+    return la * (la + 1) // 2 + lb
+
+
+# ----------------------------------------------------------------------
+# expression helpers
+# ----------------------------------------------------------------------
+class Emitter:
+    def __init__(self, indent='        '):
+        self.lines = []
+        self.ind = indent
+
+    def __call__(self, s):
+        self.lines.append(self.ind + s)
+
+    def text(self):
+        return '\n'.join(self.lines)
+
+
+def gen_vrr(em, cls, d, zero_one):
+    """Emit G_d[e][f] for e <= lij, f <= lkl; returns dict (e, f) -> expr.
+    zero_one: the value of G_d[0][0] ('1' for x and y, 'wz' for z)."""
+    lij, lkl = cls.lij, cls.lkl
+    g = {}
+    g[(0, 0)] = zero_one
+
+    def mul(a, b):
+        if a == '1':
+            return b
+        if b == '1':
+            return a
+        return f'{a} * {b}'
+
+    for e in range(lij):
+        name = f'g{d}_{e + 1}_0'
+        t = mul(f'c0{d}', g[(e, 0)])
+        if e > 0:
+            em(f'const double {name} = fma({e}.0 * b10, {g[(e - 1, 0)]}, {t});')
+        else:
+            em(f'const double {name} = {t};')
+        g[(e + 1, 0)] = name
+    for f in range(lkl):
+        for e in range(lij + 1):
+            name = f'g{d}_{e}_{f + 1}'
+            terms = mul(f'cp{d}', g[(e, f)])
+            expr = terms
+            if f > 0:
+                expr = f'fma({f}.0 * b01, {g[(e, f - 1)]}, {expr})'
+            if e > 0:
+                expr = f'fma({e}.0 * b00, {g[(e - 1, f)]}, {expr})'
+            em(f'const double {name} = {expr};')
+            g[(e, f + 1)] = name
+    return g
+
+
+def gen_root_acc(cls):
+    em = Emitter('    ')
+    gx = gen_vrr(em, cls, 'x', '1')
+    gy = gen_vrr(em, cls, 'y', '1')
+    gz = gen_vrr(em, cls, 'z', 'wz')
+    E, F = cls.eset(), cls.fset()
+    # products of x and y factors, shared between accumulators
+    uses = {}
+    for (_, ec) in E:
+        for (_, fc) in F:
+            key = (ec[0], fc[0], ec[1], fc[1])
+            uses[key] = uses.get(key, 0) + 1
+    named = {}
+    nf = len(F)
+    for ie, (_, ec) in enumerate(E):
+        for jf, (_, fc) in enumerate(F):
+            a = gx[(ec[0], fc[0])]
+            b = gy[(ec[1], fc[1])]
+            c = gz[(ec[2], fc[2])]
+            key = (ec[0], fc[0], ec[1], fc[1])
+            if a == '1' and b == '1':
+                xy = None
+            elif a == '1':
+                xy = b
+            elif b == '1':
+                xy = a
+            elif uses[key] > 1:
+                if key not in named:
+                    nm = f'xy_{key[0]}{key[1]}{key[2]}{key[3]}'
+                    em(f'const double {nm} = {a} * {b};')
+                    named[key] = nm
+                xy = named[key]
+            else:
+                xy = f'({a} * {b})'
+            k = ie * nf + jf
+            if xy is None:
+                em(f'acc[{k}] += {c};')
+            else:
+                em(f'acc[{k}] = fma({xy}, {c}, acc[{k}]);')
+    return em.text()
+
+
+def gen_row_acc(cls, f0, f1):
+    """acc[f - f0] += gx[fx] * gy[fy] * gz[fz] for f in [f0, f1)."""
+    em = Emitter('    ')
+    F = cls.fset()
+    for jf in range(f0, f1):
+        _, fc = F[jf]
+        em(f'acc[{jf - f0}] = fma(gx[{fc[0]}] * gy[{fc[1]}], gz[{fc[2]}], acc[{jf - f0}]);')
+    return em.text()
+
+
+def gen_hrr(la, lb, prefix, vec):
+    """(a, b) from levels la..la+lb of the input: out[a*nb + b] for a at
+    level la, b at level lb.  in[] is ordered level by level."""
+    em = Emitter('    ')
+    off = {}
+    o = 0
+    for L in range(la, la + lb + 1):
+        off[L] = o
+        o += ncart(L)
+    memo = {}
+
+    def val(L, a, k, b):
+        """value of the (a at level L | b at level k) intermediate."""
+        key = (L, a, k, b)
+        if key in memo:
+            return memo[key]
+        if k == 0:
+            expr = f'in[{off[L] + cidx(L, a)}]'
+            memo[key] = expr
+            return expr
+        # recurse on the first nonzero direction of b
+        d = 0 if b[0] > 0 else (1 if b[1] > 0 else 2)
+        bm = list(b)
+        bm[d] -= 1
+        bm = tuple(bm)
+        ap = list(a)
+        ap[d] += 1
+        ap = tuple(ap)
+        t1 = val(L + 1, ap, k - 1, bm)
+        t2 = val(L, a, k - 1, bm)
+        name = f'{prefix}{k}_{L}_{cidx(L, a)}_{cidx(k, b)}'
+        em(f'const double {name} = fma({vec}{"xyz"[d]}, {t2}, {t1});')
+        memo[key] = name
+        return name
+
+    na, nb = ncart(la), ncart(lb)
+    outs = []
+    for ia, a in enumerate(comps(la)):
+        for ib, b in enumerate(comps(lb)):
+            outs.append(f'out[{ia * nb + ib}] = {val(la, a, lb, b)};')
+    for s in outs:
+        em(s)
+    return em.text()
+
+
+def gen_class_header(cls):
+    E, F = cls.eset(), cls.fset()
+    lines = [f'struct Cls_{cls.tag} {{',
+             f'    static constexpr int LI = {cls.li}, LJ = {cls.lj}, '
+             f'LK = {cls.lk}, LL = {cls.ll};',
+             f'    static constexpr int LIJ = {cls.lij}, LKL = {cls.lkl}, '
+             f'NROOTS = {cls.nroots};',
+             f'    static constexpr int NI = {ncart(cls.li)}, NJ = {ncart(cls.lj)}, '
+             f'NK = {ncart(cls.lk)}, NL = {ncart(cls.ll)};',
+             f'    static constexpr int NE = {cls.ne}, NF = {cls.nf};',
+             f'    static constexpr bool REG = {"true" if cls.form == "reg" else "false"};']
+    if cls.form == 'team':
+        parts = cls.fparts()
+        lines.append(f'    static constexpr int TEAM_LANES = {cls.team_lanes}, '
+                     f'NWF = {cls.nwf}, TEAM = {cls.team_threads};')
+        lines.append(f'    static constexpr int FPART = {parts[0][1] - parts[0][0]};')
+        # e-component table: ex, ey, ez per e index
+        ex = ', '.join(str(c[0]) for _, c in E)
+        ey = ', '.join(str(c[1]) for _, c in E)
+        ez = ', '.join(str(c[2]) for _, c in E)
+        lines.append(f'    __device__ static __forceinline__ int ex(int e) '
+                     f'{{ constexpr int t[NE] = {{{ex}}}; return t[e]; }}')
+        lines.append(f'    __device__ static __forceinline__ int ey(int e) '
+                     f'{{ constexpr int t[NE] = {{{ey}}}; return t[e]; }}')
+        lines.append(f'    __device__ static __forceinline__ int ez(int e) '
+                     f'{{ constexpr int t[NE] = {{{ez}}}; return t[e]; }}')
+        for p, (f0, f1) in enumerate(parts):
+            lines.append(f'    __device__ static __forceinline__ void row_acc_{p}('
+                         'const double *gx, const double *gy, const double *gz, '
+                         'double *acc) {')
+            lines.append(gen_row_acc(cls, f0, f1))
+            lines.append('    }')
+        lines.append('    template <int P> __device__ static __forceinline__ void '
+                     'row_acc(const double *gx, const double *gy, const double *gz, '
+                     'double *acc) {')
+        for p in range(len(parts)):
+            lines.append(f'        if (P == {p}) row_acc_{p}(gx, gy, gz, acc);')
+        lines.append('    }')
+        lines.append('    template <int P> __device__ static constexpr int fbegin() {')
+        lines.append('        return ' + ' '.join(f'P == {p} ? {f0} :' for p, (f0, _) in enumerate(parts)) + ' 0;')
+        lines.append('    }')
+        lines.append('    template <int P> __device__ static constexpr int fend() {')
+        lines.append('        return ' + ' '.join(f'P == {p} ? {f1} :' for p, (_, f1) in enumerate(parts)) + ' 0;')
+        lines.append('    }')
+    else:
+        lines.append('    static constexpr int TEAM_LANES = 1, NWF = 1, TEAM = 1, FPART = NF;')
+        lines.append('    __device__ static __forceinline__ void root_acc('
+                     'double c0x, double c0y, double c0z, double cpx, double cpy, '
+                     'double cpz, double b00, double b10, double b01, double wz, '
+                     'double *acc) {')
+        lines.append(gen_root_acc(cls))
+        lines.append('    }')
+    lines.append('    __device__ static __forceinline__ void hrr_bra(const double *in, '
+                 'double *out, double ABx, double ABy, double ABz) {')
+    lines.append(gen_hrr(cls.li, cls.lj, 'hb', 'AB'))
+    lines.append('    }')
+    lines.append('    __device__ static __forceinline__ void hrr_ket(const double *in, '
+                 'double *out, double CDx, double CDy, double CDz) {')
+    lines.append(gen_hrr(cls.lk, cls.ll, 'hk', 'CD'))
+    lines.append('    }')
+    lines.append('};')
+    return '\n'.join(lines)
+
+
+def gen_unit(A, B, cls):
+    return '\n'.join([
+        '// Generated by electrolites_b200/codegen/gen_classes.py -- do not edit.',
+        '#include "../jk_kernels.cuh"',
+        '',
+        gen_class_header(cls),
+        '',
+        f'JK_DEFINE_CLASS({cls.tag}, {A}, {B})',
+        ''])
+
+
+def write_all(outdir, lmax=LMAX):
+    os.makedirs(outdir, exist_ok=True)
+    classes = all_classes(lmax)
+    written = []
+    for A, B, cls in classes:
+        path = os.path.join(outdir, f'class_{cls.tag}.cu')
+        src = gen_unit(A, B, cls)
+        old = open(path).read() if os.path.exists(path) else None
+        if old != src:
+            with open(path + '.tmp', 'w') as f:
+                f.write(src)
+            os.replace(path + '.tmp', path)
+        written.append(path)
+    # registry: declarations + table in pair-class order
+    reg = ['// Generated by electrolites_b200/codegen/gen_classes.py -- do not edit.',
+           '#pragma once',
+           '#include "../jk_launch.h"']
+    for A, B, cls in classes:
+        reg.append(f'int jk_launch_{cls.tag}(const ClassArgs &a, const LaunchCfg &cfg);')
+    reg.append(f'#define JK_NCLASSES {len(classes)}')
+    reg.append('static const ClassEntry jk_class_table[JK_NCLASSES] = {')
+    for A, B, cls in classes:
+        form = 0 if cls.form == 'reg' else 1
+        reg.append(f'    {{{A}, {B}, {cls.li}, {cls.lj}, {cls.lk}, {cls.ll}, '
+                   f'{form}, {1 if cls.form == "reg" else cls.team_threads}, '
+                   f'jk_launch_{cls.tag}}},')
+    reg.append('};')
+    with open(os.path.join(outdir, 'class_table.inc.tmp'), 'w') as f:
+        f.write('\n'.join(reg) + '\n')
+    os.replace(os.path.join(outdir, 'class_table.inc.tmp'),
+               os.path.join(outdir, 'class_table.inc'))
+    return written
+
+
+if __name__ == '__main__':
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(
+        os.path.dirname(os.path.abspath(__file__)), '..', 'csrc', 'generated')
+    for p in write_all(out):
+        print(p)

@@ -1,0 +1,22 @@
+// Host-side launch interface between the plan/build driver (jk_api.cu) and
+// the generated per-class translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include "jk_device.cuh"
+
+struct LaunchCfg {
+    cudaStream_t stream;
+    int num_sms;
+    int blocks_per_sm;     // persistent grid: num_sms * blocks_per_sm blocks
+    int mixed;             // 1: mixed-precision instantiation
+};
+
+typedef int (*ClassLauncher)(const ClassArgs &, const LaunchCfg &);
+
+struct ClassEntry {
+    int bra_class, ket_class;     // pair-class indices la*(la+1)/2 + lb
+    int li, lj, lk, ll;
+    int form;                     // 0 register form, 1 team form
+    int team_threads;
+    ClassLauncher launch;
+};

@@ -1,0 +1,246 @@
+// Preprocessing and post-processing kernels of the J/K engine:
+// primitive-pair records, Schwarz bounds, density screening table,
+// symmetrised / transposed densities and the final J/K assembly.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include "jk_device.cuh"
+
+struct ShellDev {
+    double x, y, z;
+    int l, nprim;
+    int exp_off, coef_off;   // into the device copy of exponents/coefficients
+};
+
+#define JK_PRIM_EXP_CUTOFF 60.0   // primitive pairs with a_i a_j/a_ij |AB|^2 > 60 are dropped
+
+// One record per kept primitive pair: {a_ij, K_ij, P, P - A}.
+__global__ void prim_pair_fill_kernel(const int4 *__restrict__ rec, long long nrec,
+                                      const ShellDev *__restrict__ sh,
+                                      const double *__restrict__ basis_data,
+                                      double *__restrict__ prim)
+{
+    long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    const int4 q = rec[r];
+    const ShellDev A = sh[q.x], B = sh[q.y];
+    const double ai = basis_data[A.exp_off + q.z], aj = basis_data[B.exp_off + q.w];
+    const double ci = basis_data[A.coef_off + q.z], cj = basis_data[B.coef_off + q.w];
+    const double aij = ai + aj;
+    const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
+    const double rr = abx * abx + aby * aby + abz * abz;
+    const double kij = ci * cj * exp(-ai * aj / aij * rr);
+    const double t = aj / aij;
+    double *o = prim + r * 8;
+    o[0] = aij;
+    o[1] = kij;
+    o[2] = A.x - t * abx;       // P = A + aj/aij (B - A)
+    o[3] = A.y - t * aby;
+    o[4] = A.z - t * abz;
+    o[5] = -t * abx;            // P - A
+    o[6] = -t * aby;
+    o[7] = -t * abz;
+}
+
+// ---------------------------------------------------------------------------
+// Schwarz bound per shell pair: q = log sqrt(max_ab |(ab|ab)|), with a
+// runtime-l Rys evaluation (l <= 3).  One thread per pair; O(npairs) work.
+// ---------------------------------------------------------------------------
+__device__ inline int ncart_d(int l) { return (l + 1) * (l + 2) / 2; }
+
+__device__ inline void cart_comp_d(int l, int n, int &lx, int &ly, int &lz)
+{
+    int c = 0;
+    for (int x = l; x >= 0; --x)
+        for (int y = l - x; y >= 0; --y) {
+            if (c == n) { lx = x; ly = y; lz = l - x - y; return; }
+            ++c;
+        }
+    lx = ly = lz = 0;
+}
+
+__device__ inline void rys_roots_rt(int n, double x, const double *tab, double *r, double *w)
+{
+    switch (n) {
+    case 1: rys_roots<1>(x, tab, r, w); break;
+    case 2: rys_roots<2>(x, tab, r, w); break;
+    case 3: rys_roots<3>(x, tab, r, w); break;
+    case 4: rys_roots<4>(x, tab, r, w); break;
+    case 5: rys_roots<5>(x, tab, r, w); break;
+    case 6: rys_roots<6>(x, tab, r, w); break;
+    default: rys_roots<7>(x, tab, r, w); break;
+    }
+}
+
+__global__ void schwarz_kernel(const int4 *__restrict__ pairs, int npairs,
+                               const ShellDev *__restrict__ sh,
+                               const double *__restrict__ prim,
+                               const double *__restrict__ rys, float *__restrict__ q_out)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int4 pr = pairs[p];   // ish, jsh, prim0, nprim
+    const ShellDev A = sh[pr.x], B = sh[pr.y];
+    const int li = A.l, lj = B.l, lij = li + lj;
+    const int nroots = lij + 1;
+    const int ni = ncart_d(li), nj = ncart_d(lj);
+    const double AB[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+    double diag[100];
+    for (int n = 0; n < ni * nj; ++n) diag[n] = 0.;
+    double G[7][7], Ib[4][4][7], I[3][4][4][4][4];
+    double r[7], w[7];
+    for (int kp = 0; kp < pr.w; ++kp) {
+        const double *K = prim + (size_t)(pr.z + kp) * 8;
+        const double akl = K[0];
+        for (int bp = 0; bp < pr.w; ++bp) {
+            const double *P = prim + (size_t)(pr.z + bp) * 8;
+            const double aij = P[0];
+            const double PQ[3] = {P[2] - K[2], P[3] - K[3], P[4] - K[4]};
+            const double s = aij + akl;
+            const double rr = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+            const double x = aij * akl / s * rr;
+            const double pref = JK_PI_FAC * P[1] * K[1] / (aij * akl * sqrt(s));
+            rys_roots_rt(nroots, x, rys, r, w);
+            for (int ir = 0; ir < nroots; ++ir) {
+                const double u = r[ir];
+                const double up = u * akl / s, uq = u * aij / s;
+                const double b00 = 0.5 * u / s;
+                const double b10 = 0.5 / aij * (1 - up);
+                const double b01 = 0.5 / akl * (1 - uq);
+                for (int d = 0; d < 3; ++d) {
+                    const double c0 = P[5 + d] - up * PQ[d];
+                    const double cp = K[5 + d] + uq * PQ[d];
+                    G[0][0] = d == 2 ? w[ir] * pref : 1.0;
+                    for (int e = 0; e < lij; ++e)
+                        G[e + 1][0] = c0 * G[e][0] + (e ? e * b10 * G[e - 1][0] : 0.);
+                    for (int f = 0; f < lij; ++f)
+                        for (int e = 0; e <= lij; ++e)
+                            G[e][f + 1] = cp * G[e][f] + (f ? f * b01 * G[e][f - 1] : 0.) +
+                                          (e ? e * b00 * G[e - 1][f] : 0.);
+                    for (int f = 0; f <= lij; ++f) {
+                        double t[7][4];
+                        for (int e = 0; e <= lij; ++e) t[e][0] = G[e][f];
+                        for (int b = 1; b <= lj; ++b)
+                            for (int a = 0; a <= lij - b; ++a)
+                                t[a][b] = t[a + 1][b - 1] + AB[d] * t[a][b - 1];
+                        for (int a = 0; a <= li; ++a)
+                            for (int b = 0; b <= lj; ++b) Ib[a][b][f] = t[a][b];
+                    }
+                    for (int a = 0; a <= li; ++a)
+                        for (int b = 0; b <= lj; ++b) {
+                            double t[7][4];
+                            for (int f = 0; f <= lij; ++f) t[f][0] = Ib[a][b][f];
+                            for (int dd = 1; dd <= lj; ++dd)
+                                for (int c = 0; c <= lij - dd; ++c)
+                                    t[c][dd] = t[c + 1][dd - 1] + AB[d] * t[c][dd - 1];
+                            for (int c = 0; c <= li; ++c)
+                                for (int dd = 0; dd <= lj; ++dd) I[d][a][b][c][dd] = t[c][dd];
+                        }
+                }
+                for (int ia = 0; ia < ni; ++ia) {
+                    int ax, ay, az;
+                    cart_comp_d(li, ia, ax, ay, az);
+                    for (int ib = 0; ib < nj; ++ib) {
+                        int bx, by, bz;
+                        cart_comp_d(lj, ib, bx, by, bz);
+                        diag[ia * nj + ib] += I[0][ax][bx][ax][bx] * I[1][ay][by][ay][by] *
+                                              I[2][az][bz][az][bz];
+                    }
+                }
+            }
+        }
+    }
+    double m = 0.;
+    for (int n = 0; n < ni * nj; ++n) m = fmax(m, fabs(diag[n]));
+    q_out[p] = m > 0. ? (float)(0.5 * log(m)) : -INFINITY;
+}
+
+// ---------------------------------------------------------------------------
+// dm_cond[ish][jsh] = log max |D[d][a][b]|, |D[d][b][a]| over densities and
+// the shells' AOs (symmetric by construction); and its maximum.
+// ---------------------------------------------------------------------------
+__global__ void dm_cond_kernel(const double *__restrict__ dm, int n_dm, int nao,
+                               const int *__restrict__ sh_ao, const int *__restrict__ sh_nf,
+                               int nbas, float *__restrict__ dm_cond)
+{
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nbas || j >= nbas) return;
+    const int a0 = sh_ao[i], na = sh_nf[i], b0 = sh_ao[j], nb = sh_nf[j];
+    const size_t nao2 = (size_t)nao * nao;
+    double m = 0.;
+    for (int d = 0; d < n_dm; ++d) {
+        const double *D = dm + d * nao2;
+        for (int a = 0; a < na; ++a)
+            for (int b = 0; b < nb; ++b) {
+                m = fmax(m, fabs(D[(size_t)(a0 + a) * nao + b0 + b]));
+                m = fmax(m, fabs(D[(size_t)(b0 + b) * nao + a0 + a]));
+            }
+    }
+    dm_cond[(size_t)i * nbas + j] = m > 0. ? (float)log(m) : -INFINITY;
+}
+
+__global__ void max_reduce_kernel(const float *__restrict__ v, long long n, float *__restrict__ out)
+{
+    __shared__ float s[1024];
+    float m = -INFINITY;
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) m = fmaxf(m, v[k]);
+    s[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] = fmaxf(s[threadIdx.x], s[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+// error if a pair dropped at plan time could pass the screening with this
+// density: q_drop + q_max + dm_max > log_tol
+__global__ void range_check_kernel(const float *__restrict__ dm_max, float q_drop, float q_max,
+                                   float log_tol, int *__restrict__ err)
+{
+    if (q_drop + q_max + *dm_max > log_tol) atomicCAS(err, 0, 5);
+}
+
+// out[d] = X[d] + sign * Y[d]^T, 32x32 tiles (also used with Y = X)
+__global__ void add_transpose_kernel(const double *__restrict__ X, const double *__restrict__ Y,
+                                     double sign, int nao, double *__restrict__ out)
+{
+    __shared__ double tile[32][33];
+    const size_t nao2 = (size_t)nao * nao;
+    const int d = blockIdx.z;
+    const double *x = X + d * nao2;
+    const double *y = Y + d * nao2;
+    double *o = out + d * nao2;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = bx + k, c = by + threadIdx.x;   // read Y[r][c] coalesced
+        tile[k][threadIdx.x] = (r < nao && c < nao) ? y[(size_t)r * nao + c] : 0.;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = by + k, c = bx + threadIdx.x;   // out[r][c] += sign * Y[c][r]
+        if (r < nao && c < nao)
+            o[(size_t)r * nao + c] = x[(size_t)r * nao + c] + sign * tile[threadIdx.x][k];
+    }
+}
+
+// out[d] = D[d]^T
+__global__ void transpose_kernel(const double *__restrict__ D, int nao, double *__restrict__ out)
+{
+    __shared__ double tile[32][33];
+    const size_t nao2 = (size_t)nao * nao;
+    const int d = blockIdx.z;
+    const double *x = D + d * nao2;
+    double *o = out + d * nao2;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = bx + k, c = by + threadIdx.x;
+        tile[k][threadIdx.x] = (r < nao && c < nao) ? x[(size_t)r * nao + c] : 0.;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = by + k, c = bx + threadIdx.x;
+        if (r < nao && c < nao) o[(size_t)r * nao + c] = tile[threadIdx.x][k];
+    }
+}

@@ -1,0 +1,284 @@
+"""Drop-in J/K builds on the B200 engine.
+
+Mirrors the interface the reference patches (electrolites/__init__.py:59-61,
+107): GPU4PySCF's module functions ``jk.get_jk(mol, dm, hermi, vhfopt,
+with_j, with_k, omega, verbose)``, ``jk.get_j`` and ``jk.get_k``, and the
+option object's methods ``_VHFOpt.get_jk(dms, hermi, verbose)``,
+``_VHFOpt.get_k(dms, hermi, verbose, omega, lr_factor, sr_factor)`` and
+``j_engine._VHFOpt.get_j(dms, verbose)`` (electrolites/fastjk.py:276,
+electrolites/fastk.py:642, electrolites/fastj.py:540).
+
+Semantics kept from the reference:
+  * ``dms`` is (n_dm, nao, nao) (or (nao, nao)); ``hermi`` 1 = symmetric,
+    2 = antisymmetric (J is zero, K antisymmetric), 0 = general;
+  * vj[k,l] = sum_ij (ij|kl) D[j,i], vk[i,l] = sum_jk (ij|kl) D[j,k];
+  * quartets are screened with the direct-SCF threshold of the option
+    object: kept when q_ij + q_kl + log max|D| > log(direct_scf_tol);
+  * only the full-range Coulomb operator is served (omega must be 0 or
+    None); anything else raises instead of falling back.
+
+The option-object methods work in the Cartesian AO basis of the molecule
+they were built for.  The module functions take densities in the
+molecule's own AO basis (spherical unless ``mol.cart``) and transform them.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+DEFAULT_TOL = 1e-13
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _as_int32(a):
+    return np.ascontiguousarray(np.asarray(a), dtype=np.int32)
+
+
+class VHFOpt:
+    """Plan of one molecule: shell pairs, primitive pairs, Schwarz bounds,
+    pair lists by class, all resident on the device across builds.
+
+    The counterpart of GPU4PySCF's ``jk._VHFOpt(mol, cutoff)``.
+    """
+
+    def __init__(self, mol, cutoff: float = DEFAULT_TOL, device: int | None = None):
+        self.mol = mol
+        self.direct_scf_tol = float(cutoff)
+        self.device = device
+        self._plan = None
+        self.nao = None
+
+    # ------------------------------------------------------------------
+    def build(self):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError('the J/K engine needs a CUDA device')
+        if self.device is None:
+            self.device = torch.cuda.current_device()
+        mol = self.mol
+        self._atm = _as_int32(mol._atm)
+        self._bas = _as_int32(mol._bas)
+        self._env = np.ascontiguousarray(mol._env, dtype=np.float64)
+        self._ao_loc = _as_int32(mol.ao_loc_nr(cart=True))
+        plan = ctypes.c_void_p()
+        L = _lib.lib()
+        _lib.check(L.jk_plan_create(
+            self._atm.ctypes.data, len(self._atm), self._bas.ctypes.data,
+            len(self._bas), self._env.ctypes.data, self._ao_loc.ctypes.data,
+            self.direct_scf_tol, int(self.device), ctypes.byref(plan)),
+            'jk_plan_create')
+        self._plan = plan
+        nao = ctypes.c_int()
+        npairs = ctypes.c_longlong()
+        _lib.check(L.jk_plan_info(plan, ctypes.byref(nao), ctypes.byref(npairs)),
+                   'jk_plan_info')
+        self.nao = nao.value
+        self.npairs = npairs.value
+        return self
+
+    def __del__(self):
+        try:
+            if self._plan is not None:
+                _lib.lib().jk_plan_destroy(self._plan)
+                self._plan = None
+        except Exception:
+            pass
+
+    @property
+    def plan(self):
+        if self._plan is None:
+            self.build()
+        return self._plan
+
+    # ------------------------------------------------------------------
+    def _prepare(self, dms):
+        torch = _torch()
+        if callable(dms):
+            dms = dms()
+        if not isinstance(dms, torch.Tensor):
+            dms = torch.as_tensor(dms)
+        squeeze = dms.ndim == 2
+        if squeeze:
+            dms = dms[None]
+        if dms.ndim != 3 or dms.shape[-1] != self.nao or dms.shape[-2] != self.nao:
+            raise ValueError(f'dms must be (n_dm, {self.nao}, {self.nao}); got '
+                             f'{tuple(dms.shape)}')
+        dev = torch.device('cuda', self.device)
+        dms = dms.to(device=dev, dtype=torch.float64).contiguous()
+        return dms, squeeze
+
+    def build_jk_async(self, dms, hermi=1, with_j=True, with_k=True,
+                       vj=None, vk=None, mixed_threshold=0.0, stream=None):
+        """Enqueue one build on ``stream`` (torch's current stream by default)
+        without synchronising; dms must be a contiguous float64 CUDA tensor
+        (n_dm, nao, nao).  Returns (vj, vk)."""
+        torch = _torch()
+        plan = self.plan
+        n = dms.shape[0]
+        if with_j and vj is None:
+            vj = torch.empty_like(dms)
+        if with_k and vk is None:
+            vk = torch.empty_like(dms)
+        if stream is None:
+            stream = torch.cuda.current_stream(dms.device)
+        _lib.check(_lib.lib().jk_build(
+            plan, ctypes.c_void_p(dms.data_ptr()), n, int(hermi), int(bool(with_j)),
+            int(bool(with_k)), ctypes.c_void_p(vj.data_ptr() if with_j else 0),
+            ctypes.c_void_p(vk.data_ptr() if with_k else 0), float(mixed_threshold),
+            ctypes.c_void_p(stream.cuda_stream)), 'jk_build')
+        return vj, vk
+
+    def sync(self, stream=None):
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(torch.device('cuda', self.device))
+        _lib.check(_lib.lib().jk_sync(self.plan, ctypes.c_void_p(stream.cuda_stream)),
+                   'jk_sync')
+
+    def get_jk(self, dms, hermi=1, verbose=None, with_j=True, with_k=True,
+               mixed_threshold=0.0):
+        """(vj, vk) as CUDA tensors shaped like dms (Cartesian AO basis)."""
+        dms, squeeze = self._prepare(dms)
+        vj, vk = self.build_jk_async(dms, hermi, with_j, with_k,
+                                     mixed_threshold=mixed_threshold)
+        self.sync()
+        if squeeze:
+            vj = vj[0] if vj is not None else None
+            vk = vk[0] if vk is not None else None
+        return vj, vk
+
+    def get_k(self, dms, hermi=1, verbose=None, omega=None, lr_factor=None,
+              sr_factor=None):
+        _check_omega(omega)
+        _, vk = self.get_jk(dms, hermi, verbose, with_j=False, with_k=True)
+        if lr_factor is not None and sr_factor is not None and lr_factor != sr_factor:
+            raise NotImplementedError('mixed-range exchange is not served')
+        if lr_factor is not None and lr_factor != 1.0:
+            vk = vk * lr_factor
+        return vk
+
+    def get_j(self, dms, verbose=None, hermi=1):
+        vj, _ = self.get_jk(dms, hermi, verbose, with_j=True, with_k=False)
+        return vj
+
+    def class_counts(self):
+        """{(li, lj, lk, ll): (quartets, primitive quartets)} evaluated by the
+        last build."""
+        L = _lib.lib()
+        ncls = ctypes.c_int()
+        _lib.check(L.jk_last_counts(self.plan, None, None, 0, ctypes.byref(ncls)),
+                   'jk_last_counts')
+        q = (ctypes.c_ulonglong * ncls.value)()
+        pq = (ctypes.c_ulonglong * ncls.value)()
+        _lib.check(L.jk_last_counts(self.plan, q, pq, ncls.value, ctypes.byref(ncls)),
+                   'jk_last_counts')
+        out = {}
+        for k in range(ncls.value):
+            ls = [ctypes.c_int() for _ in range(5)]
+            _lib.check(L.jk_class_info(k, *[ctypes.byref(x) for x in ls]), 'jk_class_info')
+            key = tuple(x.value for x in ls[:4])
+            out[key] = (int(q[k]), int(pq[k]))
+        return out
+
+    def set_timing(self, enable=True):
+        _lib.check(_lib.lib().jk_set_timing(self.plan, int(bool(enable))), 'jk_set_timing')
+
+    def last_class_ms(self):
+        """({(li, lj, lk, ll): ms of that class kernel in the last build},
+        number of kernels the last build launched)."""
+        L = _lib.lib()
+        n = 64
+        ms = (ctypes.c_float * n)()
+        launches = ctypes.c_int()
+        _lib.check(L.jk_last_class_ms(self.plan, ms, n, ctypes.byref(launches)),
+                   'jk_last_class_ms')
+        out = {}
+        for k in range(n):
+            ls = [ctypes.c_int() for _ in range(5)]
+            if L.jk_class_info(k, *[ctypes.byref(x) for x in ls]) != 0:
+                break
+            if ms[k] > 0:
+                out[tuple(x.value for x in ls[:4])] = float(ms[k])
+        return out, launches.value
+
+    def q_cond(self):
+        nb = len(self._bas)
+        q = np.zeros((nb, nb), dtype=np.float32)
+        _lib.check(_lib.lib().jk_plan_q_cond(
+            self.plan, q.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nb),
+            'jk_plan_q_cond')
+        return q
+
+
+def _check_omega(omega):
+    if omega is not None and omega != 0:
+        raise NotImplementedError('only the full-range Coulomb operator is '
+                                  'served (omega = 0)')
+
+
+# ----------------------------------------------------------------------
+# module-level functions (GPU4PySCF's jk.get_jk / get_j / get_k)
+# ----------------------------------------------------------------------
+_OPTS = {}
+
+
+def _opt_for(mol, vhfopt):
+    if vhfopt is not None:
+        return vhfopt
+    key = id(mol)
+    opt = _OPTS.get(key)
+    if opt is None or opt.mol is not mol:
+        opt = VHFOpt(mol, getattr(mol, 'direct_scf_tol', DEFAULT_TOL)).build()
+        _OPTS[key] = opt
+    return opt
+
+
+def _to_cart(mol, dms):
+    torch = _torch()
+    if getattr(mol, 'cart', False):
+        return dms, None
+    c = torch.as_tensor(mol.cart2sph_coeff(), dtype=torch.float64, device=dms.device)
+    return c @ dms @ c.T, c
+
+
+def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None,
+           verbose=None):
+    """(vj, vk) for densities in mol's AO basis.  numpy in -> numpy out;
+    torch in -> torch out."""
+    torch = _torch()
+    _check_omega(omega)
+    was_numpy = not isinstance(dm, torch.Tensor) and not hasattr(dm, '__cuda_array_interface__')
+    opt = _opt_for(mol, vhfopt)
+    d = torch.as_tensor(np.asarray(dm) if was_numpy else dm)
+    squeeze = d.ndim == 2
+    if squeeze:
+        d = d[None]
+    d = d.to(device=torch.device('cuda', opt.device), dtype=torch.float64)
+    dc, c = _to_cart(mol, d)
+    vj, vk = opt.get_jk(dc.contiguous(), hermi, verbose, with_j, with_k)
+    outs = []
+    for v in (vj, vk):
+        if v is None:
+            outs.append(None)
+            continue
+        if c is not None:
+            v = c.T @ v @ c
+        if squeeze:
+            v = v[0]
+        outs.append(v.cpu().numpy() if was_numpy else v)
+    return tuple(outs)
+
+
+def get_j(mol, dm, hermi=1, vhfopt=None, verbose=None):
+    return get_jk(mol, dm, hermi, vhfopt, True, False, None, verbose)[0]
+
+
+def get_k(mol, dm, hermi=1, vhfopt=None, omega=None, verbose=None):
+    return get_jk(mol, dm, hermi, vhfopt, False, True, omega, verbose)[1]

@@ -1,0 +1,135 @@
+/*
+ * C ABI of the B200 direct-SCF Coulomb/exchange (J/K) engine,
+ * libjk_b200.so.
+ *
+ * Every entry point returns 0 on success and a non-zero JK_ERR_* code
+ * otherwise; jk_last_error() gives the message of the last failure on the
+ * calling thread.  There is no fallback path: a shell the engine cannot
+ * handle (l > 3) or a density out of the plan's range is an error.
+ *
+ * Conventions
+ *   - Molecules are passed in PySCF's integer/float layout: atm[natm][6],
+ *     bas[nbas][8], env[] (the arrays of a pyscf.gto.Mole: _atm, _bas,
+ *     _env).  Contraction coefficients in env carry PySCF's radial
+ *     normalisation; the s/p angular factor of libcint is applied here.
+ *   - Densities and results are row-major (n, nao, nao) float64 arrays in
+ *     the Cartesian AO basis, AO order given by ao_loc (PySCF's
+ *     mol.ao_loc_nr(cart=True)); general contractions are expanded
+ *     contraction-major, as PySCF orders them.
+ *   - vj[k,l] = sum_ij (ij|kl) D[j,i],  vk[i,l] = sum_jk (ij|kl) D[j,k]
+ *     (PySCF's dot_eri_dm conventions).  hermi = 1: D symmetric; hermi = 2:
+ *     D antisymmetric (vj is zero); hermi = 0: no symmetry.
+ *   - Device pointers unless a name says _host.  Calls are asynchronous on
+ *     the given stream (NULL: the default stream); jk_sync() waits and
+ *     returns a device-side error, if any.
+ *   - One plan per stream at a time; a plan reuses its device workspace
+ *     across calls (one SCF cycle after another).
+ */
+#ifndef JK_B200_H
+#define JK_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JK_OK 0
+#define JK_ERR_ARG 1          /* invalid argument                         */
+#define JK_ERR_UNSUPPORTED 2  /* shell type the engine does not handle     */
+#define JK_ERR_CUDA 3         /* CUDA runtime error                        */
+#define JK_ERR_NOMEM 4        /* device allocation failed                  */
+#define JK_ERR_RANGE 5        /* density beyond the plan's screening range */
+#define JK_ERR_DEVICE 6       /* error flag raised inside a kernel         */
+
+typedef struct jk_plan jk_plan;
+
+/*
+ * Build a plan: shell-pair and primitive-pair tables, Schwarz bounds
+ * q_ij = log sqrt(max |(ij|ij)|), pair lists by angular-momentum class
+ * sorted by q.  direct_scf_tol is the screening threshold of every later
+ * build (PySCF's mol.direct_scf_tol; quartets are kept when
+ * q_ij + q_kl + log max|D_block| > log(tol)).  device: CUDA ordinal.
+ *
+ * Replaces the plan GPU4PySCF's _VHFOpt.build() prepares and the
+ * reference's per-call screening prep: electrolites/fastk.py:336-351 (_prep),
+ * electrolites/compat.py:54-78 (dense_q_cond) and :84-149
+ * (tril_pair_mappings).
+ */
+int jk_plan_create(const int *atm, int natm, const int *bas, int nbas,
+                   const double *env, const int *ao_loc,
+                   double direct_scf_tol, int device, jk_plan **out);
+
+int jk_plan_destroy(jk_plan *plan);
+
+/* nao (Cartesian) and the number of shell pairs kept by the plan. */
+int jk_plan_info(const jk_plan *plan, int *nao, long long *npairs);
+
+/*
+ * J and/or K for n_dm densities dm[n_dm][nao][nao] (device).  vj and vk
+ * (device, [n_dm][nao][nao]) are overwritten; either may be NULL when
+ * with_j / with_k is 0.  mixed_threshold <= 0 gives the plain all-FP64
+ * build; > 0 runs quartets whose screened bound
+ * |(ij|ij)|^1/2 |(kl|kl)|^1/2 max|D| is below it with FP32 Rys evaluation
+ * (FP64 accumulation).
+ *
+ * Replaces _VHFOpt.get_jk / get_k and j_engine._VHFOpt.get_j as the
+ * reference patches them: electrolites/fastjk.py:276-357 (get_jk),
+ * electrolites/fastk.py:642-741 (get_k), electrolites/fastj.py:540-569
+ * (get_j_181), including their hermi post-processing.
+ */
+int jk_build(jk_plan *plan, const double *dm, int n_dm, int hermi,
+             int with_j, int with_k, double *vj, double *vk,
+             double mixed_threshold, void *stream);
+
+/*
+ * The same with host buffers: copies dm in, builds, copies vj/vk out, and
+ * synchronises.  The call a CPU-side caller (PySCF's own get_jk) makes.
+ */
+int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi,
+                  int with_j, int with_k, double *vj_host, double *vk_host,
+                  double mixed_threshold, void *stream);
+
+/* Wait for the plan's work on stream; returns JK_ERR_DEVICE if a kernel
+ * raised its error flag (the flag is then cleared). */
+int jk_sync(jk_plan *plan, void *stream);
+
+/*
+ * Shell quartets and primitive quartets evaluated by the last build, per
+ * angular-momentum class (index k of jk_class_info), and the number of
+ * classes.  Either array may be NULL.  Synchronises the stream of the last
+ * build.
+ */
+int jk_last_counts(jk_plan *plan, unsigned long long *quartets,
+                   unsigned long long *prim_quartets, int ncounts,
+                   int *nclasses);
+
+/* li, lj, lk, ll and the form (0 register, 1 team) of class k. */
+int jk_class_info(int k, int *li, int *lj, int *lk, int *ll, int *form);
+
+/*
+ * Per-class kernel timing.  With enable = 1 every later build records CUDA
+ * events around each class kernel on the build's stream;
+ * jk_last_class_ms() then returns the milliseconds of each class kernel of
+ * the last build (0 for classes not launched) and the number of kernels the
+ * library launched in that build.  Synchronises the last build's stream.
+ */
+int jk_set_timing(jk_plan *plan, int enable);
+int jk_last_class_ms(jk_plan *plan, float *ms, int ncounts, int *launches);
+
+/*
+ * Measurement helper, no counterpart in the reference: the FP64 FMA
+ * throughput of the device (TFLOP/s, 2 flops per FMA) from a
+ * register-resident FMA chain on every SM, timed with CUDA events.
+ */
+int jk_fp64_peak(int device, double *tflops);
+
+/* Schwarz bounds q[nbas][nbas] (host, float, -inf for pairs below the
+ * plan's range), in the caller's shell numbering when no shell has a
+ * general contraction. */
+int jk_plan_q_cond(const jk_plan *plan, float *q_host, int nbas);
+
+const char *jk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

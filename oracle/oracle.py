@@ -1,0 +1,129 @@
+"""ctypes wrapper of the CPU oracle (jk_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by bench.py's CPU-baseline leg, as the checker.  The product package never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, '_build', 'libjk_oracle.so')
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(['make', '-s', '-C', HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.oracle_rys.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
+        L.oracle_eri_shells.argtypes = [ip, ip, dp, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, dp]
+        L.oracle_q_cond.argtypes = [ip, ip, ctypes.c_int, dp, dp]
+        L.oracle_jk.argtypes = [ip, ip, ctypes.c_int, dp, ip, dp, ctypes.c_int,
+                                ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                dp, dp, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_longlong)]
+        L.oracle_jk_sample.argtypes = L.oracle_jk.argtypes + [
+            ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong]
+        _lib = L
+    return _lib
+
+
+def _p(a, t=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _arrays(mol):
+    atm = np.ascontiguousarray(mol._atm, dtype=np.int32)
+    bas = np.ascontiguousarray(mol._bas, dtype=np.int32)
+    env = np.ascontiguousarray(mol._env, dtype=np.float64)
+    return atm, bas, env
+
+
+def rys(n: int, x: float):
+    r = np.zeros(n)
+    w = np.zeros(n)
+    if lib().oracle_rys(n, float(x), _p(r), _p(w)):
+        raise ValueError('bad Rys order')
+    return r, w
+
+
+def eri_shells(mol, i, j, k, l):
+    from electrolites_b200.gto import ncart
+    atm, bas, env = _arrays(mol)
+    ls = [int(mol._bas[s, 1]) for s in (i, j, k, l)]
+    out = np.zeros([ncart(x) for x in ls])
+    if lib().oracle_eri_shells(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                               _p(env), i, j, k, l, _p(out)):
+        raise ValueError('unsupported shell')
+    return out
+
+
+def q_cond(mol):
+    atm, bas, env = _arrays(mol)
+    q = np.zeros((mol.nbas, mol.nbas))
+    lib().oracle_q_cond(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                        mol.nbas, _p(env), _p(q))
+    return q
+
+
+def jk(mol, dms, tol=1e-13, with_j=True, with_k=True, nthreads=0):
+    """(vj, vk, n_quartets) for Cartesian-AO densities dms (n_dm, nao, nao);
+    tol <= 0 disables screening."""
+    atm, bas, env = _arrays(mol)
+    dms = np.ascontiguousarray(dms, dtype=np.float64)
+    squeeze = dms.ndim == 2
+    if squeeze:
+        dms = dms[None]
+    ao_loc = np.ascontiguousarray(mol.ao_loc_nr(cart=True), dtype=np.int32)
+    vj = np.zeros_like(dms)
+    vk = np.zeros_like(dms)
+    nq = ctypes.c_longlong(0)
+    err = lib().oracle_jk(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                          mol.nbas, _p(env), _p(ao_loc, ctypes.c_int),
+                          _p(dms), dms.shape[0], float(tol), int(with_j),
+                          int(with_k), _p(vj), _p(vk), int(nthreads),
+                          ctypes.byref(nq))
+    if err:
+        raise RuntimeError(f'oracle_jk failed ({err})')
+    if squeeze:
+        vj, vk = vj[0], vk[0]
+    return vj, vk, nq.value
+
+
+def jk_sample(mol, dms, ij_list, tol=1e-13, with_j=True, with_k=True, nthreads=0):
+    """oracle J/K restricted to the bra shell pairs ij_list (linear index
+    i*(i+1)/2 + j); returns (vj, vk, n_quartets)."""
+    atm, bas, env = _arrays(mol)
+    dms = np.ascontiguousarray(dms, dtype=np.float64)
+    if dms.ndim == 2:
+        dms = dms[None]
+    ao_loc = np.ascontiguousarray(mol.ao_loc_nr(cart=True), dtype=np.int32)
+    ij = np.ascontiguousarray(ij_list, dtype=np.int64)
+    vj = np.zeros_like(dms)
+    vk = np.zeros_like(dms)
+    nq = ctypes.c_longlong(0)
+    err = lib().oracle_jk_sample(
+        _p(atm, ctypes.c_int), _p(bas, ctypes.c_int), mol.nbas, _p(env),
+        _p(ao_loc, ctypes.c_int), _p(dms), dms.shape[0], float(tol), int(with_j),
+        int(with_k), _p(vj), _p(vk), int(nthreads), ctypes.byref(nq),
+        _p(ij, ctypes.c_longlong), len(ij))
+    if err:
+        raise RuntimeError(f'oracle_jk_sample failed ({err})')
+    return vj, vk, nq.value

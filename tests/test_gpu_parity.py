@@ -1,0 +1,208 @@
+"""Parity of the CUDA J/K engine with the CPU oracle (through the C ABI).
+
+Tolerances (plain FP64 form): every J/K element within 1e-10 absolute of
+the oracle, and the J and K energies within 1e-9 Eh.  Shapes of the
+reference's own tests (tests/test_jk.py:91-115 there): identical densities
+must give identical results, random perturbations exercise the union
+screening, atom-local densities the CPHF shape; hermi 1, 0 and 2; several
+densities per call; an all-zero density must return zeros."""
+import os
+
+import numpy as np
+import pytest
+
+from electrolites_b200 import clusters
+from electrolites_b200.gto import Mole
+
+pytestmark = pytest.mark.gpu
+
+ATOL = 1e-10
+ETOL = 1e-9
+TOL = 1e-13
+GOLD = os.path.join(os.path.dirname(__file__), 'golden', 'h2o8_631gs_oracle.npz')
+
+
+@pytest.fixture(scope='module')
+def torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    return torch
+
+
+def all_class_mol():
+    """Three centres carrying s, p, d and f shells of one and two
+    primitives: every one of the 55 classes up to (ff|ff) occurs."""
+    b = {
+        'H': [[0, (1.3, 0.6), (0.3, 0.5)], [1, (0.9, 1.0)], [2, (0.7, 1.0)], [3, (0.6, 1.0)]],
+        'He': [[0, (0.8, 1.0)], [1, (1.4, 0.7), (0.4, 0.4)], [2, (1.1, 1.0)], [3, (0.9, 1.0)]],
+        'C': [[0, (2.1, 1.0)], [1, (0.5, 1.0)], [2, (0.9, 0.5), (0.35, 0.6)], [3, (1.2, 1.0)]],
+    }
+    atom = [('H', (0.0, 0.0, 0.0)), ('He', (0.9, 0.3, -0.4)), ('C', (-0.5, 1.1, 0.6))]
+    return Mole(atom, basis=b, cart=True)
+
+
+MOLS = {
+    'h2o_631gs': lambda: clusters.water_mole(1, 3.0, 7, basis='6-31g*'),
+    'h2o2_svp': lambda: clusters.water_mole(2, 4.5, 8, basis='def2-svp'),
+    'h2o_tzvp': lambda: clusters.water_mole(1, 3.0, 9, basis='def2-tzvp'),
+    'spdf': all_class_mol,
+}
+
+
+def densities(mol, kind, n_dm, hermi, rng):
+    nao = mol.nao_cart
+    base = clusters.atomic_density(mol, 11) if kind != 'atomic' else None
+    out = np.empty((n_dm, nao, nao))
+    for i in range(n_dm):
+        if kind == 'same':
+            out[i] = base
+        elif kind == 'random':
+            out[i] = base + 1e-2 * rng.standard_normal((nao, nao)) * 10. ** -(i % 3)
+        else:
+            out[i] = 0
+            p0, p1 = mol.aoslice_by_atom(cart=True)[i % mol.natm][2:]
+            out[i, p0:p1, p0:p1] = rng.standard_normal((p1 - p0, p1 - p0))
+    if hermi == 1:
+        out = out + out.transpose(0, 2, 1)
+    elif hermi == 2:
+        out = out - out.transpose(0, 2, 1)
+    return out
+
+
+def _energies(D, vj, vk):
+    return 0.5 * np.einsum('nij,nji->', D, vj), -0.25 * np.einsum('nij,nji->', D, vk)
+
+
+def _check(torch, opt, oracle, mol, dms, hermi, with_j=True, with_k=True):
+    vj, vk = opt.get_jk(torch.as_tensor(dms), hermi, with_j=with_j, with_k=with_k)
+    rj, rk, _ = oracle.jk(mol, dms, tol=TOL)
+    if hermi == 2:
+        rj = np.zeros_like(rj)
+    if with_j:
+        gj = vj.cpu().numpy()
+        assert np.abs(gj - rj).max() <= ATOL, np.abs(gj - rj).max()
+    if with_k:
+        gk = vk.cpu().numpy()
+        assert np.abs(gk - rk).max() <= ATOL, np.abs(gk - rk).max()
+    if with_j and with_k:
+        ej, ek = _energies(dms, gj, gk)
+        rej, rek = _energies(dms, rj, rk)
+        assert abs(ej - rej) <= ETOL and abs(ek - rek) <= ETOL
+    return vj, vk
+
+
+@pytest.mark.parametrize('name', list(MOLS))
+@pytest.mark.parametrize('hermi', [1, 0, 2])
+def test_parity_small(torch, oracle, name, hermi):
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS[name]()
+    opt = VHFOpt(mol, TOL).build()
+    rng = np.random.default_rng(20240908)
+    for kind, n_dm in [('random', 1), ('random', 3), ('atomic', 2)]:
+        dms = densities(mol, kind, n_dm, hermi, rng)
+        _check(torch, opt, oracle, mol, dms, hermi)
+
+
+@pytest.mark.parametrize('with_j,with_k', [(True, False), (False, True)])
+def test_parity_j_only_k_only(torch, oracle, with_j, with_k):
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS['spdf']()
+    opt = VHFOpt(mol, TOL).build()
+    dms = densities(mol, 'random', 2, 1, np.random.default_rng(3))
+    _check(torch, opt, oracle, mol, dms, 1, with_j, with_k)
+
+
+def test_same_densities_identical(torch):
+    """Identical densities come back identical (a wrong per-density stride
+    cannot hide); differences are FP64 atomic-order round-off only."""
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS['h2o2_svp']()
+    opt = VHFOpt(mol, TOL).build()
+    dms = densities(mol, 'same', 4, 1, np.random.default_rng(0))
+    vj, vk = opt.get_jk(torch.as_tensor(dms), 1)
+    for v in (vj, vk):
+        v = v.cpu().numpy()
+        assert np.abs(v - v[0]).max() <= 1e-13 * np.abs(v).max()
+
+
+def test_zero_density_returns_zeros(torch):
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS['h2o_631gs']()
+    opt = VHFOpt(mol, TOL).build()
+    z = torch.zeros((2, mol.nao_cart, mol.nao_cart), dtype=torch.float64)
+    vj, vk = opt.get_jk(z, 1)
+    assert float(vj.abs().max()) == 0.0 and float(vk.abs().max()) == 0.0
+
+
+def test_schwarz_bounds(torch, oracle):
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS['spdf']()
+    opt = VHFOpt(mol, TOL).build()
+    q = opt.q_cond()
+    ref = oracle.q_cond(mol)
+    np.testing.assert_allclose(q, ref, rtol=0, atol=2e-6)
+
+
+def test_cpu_workload_against_fixture(torch):
+    """(H2O)_8 / 6-31G* shapes, atom-block density: the CPU-runnable
+    workload, against the oracle's committed J/K."""
+    from electrolites_b200.jk import VHFOpt
+    g = np.load(GOLD)
+    mol = clusters.water_mole(8, 7.0, int(g['seed']), basis='6-31g*')
+    D = g['dm']
+    opt = VHFOpt(mol, float(g['tol'])).build()
+    vj, vk = opt.get_jk(torch.as_tensor(D), 1)
+    vj, vk = vj.cpu().numpy(), vk.cpu().numpy()
+    assert np.abs(vj - g['vj']).max() <= ATOL
+    assert np.abs(vk - g['vk']).max() <= ATOL
+    ej, ek = _energies(D[None], vj[None], vk[None])
+    rej, rek = _energies(D[None], g['vj'][None], g['vk'][None])
+    assert abs(ej - rej) <= ETOL and abs(ek - rek) <= ETOL
+    nq = sum(v[0] for v in opt.class_counts().values())
+    assert abs(nq - int(g['nquartets'])) <= 1e-3 * int(g['nquartets'])
+
+
+def test_module_functions_spherical(torch, oracle):
+    """get_jk(mol, dm) on a spherical-AO molecule: numpy in, numpy out,
+    through the Cartesian transform."""
+    from electrolites_b200 import jk
+    mol = clusters.water_mole(1, 3.0, 4, basis='6-31g*', cart=False)
+    C = mol.cart2sph_coeff()
+    rng = np.random.default_rng(1)
+    Ds = rng.standard_normal((mol.nao, mol.nao)) * 0.05
+    Ds = Ds + Ds.T
+    vj, vk = jk.get_jk(mol, Ds, hermi=1)
+    assert isinstance(vj, np.ndarray) and vj.shape == Ds.shape
+    rj, rk, _ = oracle.jk(mol, C @ Ds @ C.T, tol=TOL)
+    np.testing.assert_allclose(vj, C.T @ rj @ C, atol=ATOL)
+    np.testing.assert_allclose(vk, C.T @ rk @ C, atol=ATOL)
+    np.testing.assert_allclose(jk.get_k(mol, Ds), vk, atol=1e-14)
+
+
+def test_unsupported_requests_raise(torch):
+    from electrolites_b200 import jk
+    from electrolites_b200._lib import JKError
+    mol = MOLS['h2o_631gs']()
+    with pytest.raises(NotImplementedError):
+        jk.get_k(mol, np.eye(mol.nao), omega=0.3)
+    g = Mole([('H', (0, 0, 0))], basis={'H': [[4, (1.0, 1.0)]]}, cart=True)
+    with pytest.raises(JKError, match='unsupported'):
+        jk.VHFOpt(g).build()
+
+
+def test_host_buffer_entry_point(torch, oracle):
+    """jk_build_host: host density in, host J/K out."""
+    import ctypes
+    from electrolites_b200 import _lib
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS['h2o_tzvp']()
+    opt = VHFOpt(mol, TOL).build()
+    dms = densities(mol, 'random', 2, 1, np.random.default_rng(5))
+    vj = np.zeros_like(dms)
+    vk = np.zeros_like(dms)
+    _lib.check(_lib.lib().jk_build_host(opt.plan, dms.ctypes.data, 2, 1, 1, 1,
+                                        vj.ctypes.data, vk.ctypes.data, 0.0, None),
+               'jk_build_host')
+    rj, rk, _ = oracle.jk(mol, dms, tol=TOL)
+    assert np.abs(vj - rj).max() <= ATOL and np.abs(vk - rk).max() <= ATOL

@@ -1,0 +1,146 @@
+"""Host-side logic: basis shapes and normalisation, cluster geometry,
+densities, the Cartesian->spherical transform, the C-ABI library exports,
+the patch registry, and the flop model."""
+import ctypes
+import os
+import re
+import sys
+import types
+
+import numpy as np
+import pytest
+
+from electrolites_b200 import basis_synth, clusters, gto
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize('basis,nsh,ncart,nsph', [('6-31g*', 10, 19, 18),
+                                                  ('def2-svp', 12, 25, 24),
+                                                  ('def2-tzvp', 19, 48, 43)])
+def test_basis_shapes(basis, nsh, ncart, nsph):
+    mol = clusters.water_mole(1, 3.0, 1, basis=basis)
+    assert mol.nbas == nsh
+    assert mol.nao_cart == ncart
+    assert mol.ao_loc_nr(cart=False)[-1] == nsph
+
+
+def test_normalisation():
+    mol = clusters.water_mole(1, 3.0, 2, basis='def2-tzvp')
+    S = mol.intor_ovlp_cart()
+    loc = mol.ao_loc_nr(True)
+    for ish, l in enumerate(mol._bas[:, 1]):
+        if l < 2:   # s and p Cartesian functions are normalised
+            d = np.diag(S)[loc[ish]:loc[ish + 1]]
+            np.testing.assert_allclose(d, 1.0, rtol=1e-12)
+    C = mol.cart2sph_coeff()
+    Ssph = C.T @ S @ C
+    np.testing.assert_allclose(np.diag(Ssph), 1.0, rtol=1e-10)
+
+
+def test_cluster_geometry():
+    atoms = clusters.water_cluster(24, 3.1 * 24 ** (1 / 3), 42)
+    O = np.array([xyz for s, xyz in atoms if s == 'O'])
+    d = np.linalg.norm(O[:, None] - O[None], axis=-1) + np.eye(len(O)) * 99
+    assert d.min() >= 2.7
+    H = np.array([xyz for s, xyz in atoms if s == 'H']).reshape(-1, 2, 3)
+    np.testing.assert_allclose(np.linalg.norm(H - O[:, None], axis=-1), 0.9572, rtol=1e-12)
+    v1, v2 = H[:, 0] - O, H[:, 1] - O
+    ang = np.degrees(np.arccos(np.sum(v1 * v2, 1) / 0.9572 ** 2))
+    np.testing.assert_allclose(ang, 104.52, rtol=1e-10)
+    assert clusters.water_cluster(24, 3.1 * 24 ** (1 / 3), 42) == atoms   # seeded
+
+
+def test_density_electron_count():
+    mol = clusters.water_mole(3, 5.0, 3)
+    D = clusters.atomic_density(mol, 3)
+    S = mol.intor_ovlp_cart()
+    assert abs(np.trace(D @ S) - 30) < 1e-10
+    np.testing.assert_allclose(D, D.T, atol=1e-14)
+    da, db = clusters.uhf_pair(D, 5)
+    np.testing.assert_allclose(da, 0.5 * D)
+    np.testing.assert_allclose(db, db.T, atol=1e-15)
+    assert 0 < np.abs(db - da).max() < 0.02 * np.abs(da).max()
+
+
+def _header_symbols():
+    text = open(os.path.join(ROOT, 'include', 'jk_b200.h')).read()
+    return sorted(set(re.findall(r'^\s*(?:int|const char \*)\s*(jk_\w+)\s*\(', text, re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    from electrolites_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip('library not built')
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    syms = _header_symbols()
+    assert 'jk_build' in syms and 'jk_plan_create' in syms
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) <= set(_lib.EXPORTS)
+
+
+def test_library_errors_without_device_or_bad_args():
+    """Argument errors come back as codes with a message; no silent path."""
+    from electrolites_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip('library not built')
+    L = _lib.lib()
+    plan = ctypes.c_void_p()
+    rc = L.jk_plan_create(None, 0, None, 0, None, None, 1e-13, 0, ctypes.byref(plan))
+    assert rc != 0 and plan.value is None
+    assert len(L.jk_last_error()) > 0
+    assert L.jk_build(None, None, 1, 1, 1, 1, None, None, 0.0, None) == 1
+
+
+def test_package_fails_loudly_without_library(monkeypatch):
+    from electrolites_b200 import _lib
+    monkeypatch.setattr(_lib, 'LIB_PATH', '/nonexistent/libjk_b200.so')
+    monkeypatch.setattr(_lib, '_lib', None)
+    with pytest.raises(RuntimeError, match='not built'):
+        _lib.lib()
+
+
+def test_patch_registry(monkeypatch):
+    import electrolites_b200 as eb
+    status = eb.check_targets()
+    assert set(status) == set(eb.MODULES)
+    if any(v is not None for v in status.values()):
+        with pytest.raises(ImportError):
+            eb.patch('fastjk')
+    # a stand-in for gpu4pyscf's option classes
+    pkg = types.ModuleType('gpu4pyscf')
+    scf = types.ModuleType('gpu4pyscf.scf')
+    jkm = types.ModuleType('gpu4pyscf.scf.jk')
+    jem = types.ModuleType('gpu4pyscf.scf.j_engine')
+
+    class Opt:
+        def get_jk(self, dms, hermi, verbose=None):
+            return 'orig'
+
+        def get_k(self, dms, hermi, verbose=None, omega=None, lr_factor=None, sr_factor=None):
+            return 'orig'
+
+    class OptJ:
+        def get_j(self, dms, verbose=None):
+            return 'orig'
+
+    jkm._VHFOpt, jem._VHFOpt = Opt, OptJ
+    for name, m in [('gpu4pyscf', pkg), ('gpu4pyscf.scf', scf), ('gpu4pyscf.scf.jk', jkm),
+                    ('gpu4pyscf.scf.j_engine', jem)]:
+        monkeypatch.setitem(sys.modules, name, m)
+    monkeypatch.setattr(eb, '_PATCHED', {})
+    assert all(v is None for v in eb.check_targets().values())
+    with pytest.raises(KeyError):
+        eb.patch('nope')
+    eb.patch_all()
+    assert eb.patched() == sorted(eb.MODULES)
+    assert Opt.get_jk is eb._get_jk and OptJ.get_j is eb._get_j
+
+
+def test_flop_model_counts():
+    from electrolites_b200 import flop_model as F
+    # (ss|ss), 1x1 primitives, 1 density, J+K
+    f = F.quartet_flops(0, 0, 0, 0, 1, 1, n_j=1, n_k=1)
+    assert f == F.F_PRIM_BASE + 1 * (F.F_ROOT + 3 * F.f_2d(0, 0, 0, 0) + 3 * 1) + 1 * 1 * 2 * 6
+    assert F.quartet_flops(2, 2, 2, 2, 1, 1, 1, 1) > F.quartet_flops(1, 1, 1, 1, 1, 1, 1, 1)

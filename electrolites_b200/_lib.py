@@ -49,6 +49,7 @@ def lib():
     L.jk_build_host.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, vp]
     L.jk_sync.argtypes = [vp, vp]
     L.jk_last_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong),
+                                 ctypes.POINTER(ctypes.c_ulonglong),
                                  ctypes.POINTER(ctypes.c_ulonglong), c_int, ip]
     L.jk_class_info.argtypes = [c_int, ip, ip, ip, ip, ip]
     L.jk_plan_q_cond.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int]

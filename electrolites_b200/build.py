@@ -100,6 +100,10 @@ def build(jobs: int = 0, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f'link failed:\n{r.stderr[-4000:]}')
     os.replace(tmp, LIB)
+    keep = {os.path.basename(o) for o in objs}
+    for f in os.listdir(OBJ):
+        if f.endswith('.o') and f not in keep:
+            os.unlink(os.path.join(OBJ, f))
     return LIB
 
 

@@ -4,7 +4,9 @@ For every quartet class (li lj | lk ll) with li >= lj, lk >= ll and the bra
 pair class >= the ket pair class (55 classes up to f), this writes one CUDA
 translation unit under csrc/generated/ holding
 
-  * a `Cls_<li><lj><lk><ll>` struct of straight-line device functions:
+  * a `Cls_<li><lj><lk><ll>` struct of straight-line device functions,
+    templated on the arithmetic type T (double for the plain form, float for
+    the single-precision quartets of the mixed form):
       - `root_acc`: one Rys root's 2D integrals G_d[e][f] (VRR on centres i
         and k, e <= li+lj, f <= lk+ll) and the accumulation of the
         (e0|f0) Cartesian integrals, all in registers (register form);
@@ -12,7 +14,7 @@ translation unit under csrc/generated/ holding
         three rows of 2D integrals (team form, rows staged in shared memory);
       - `hrr_bra` / `hrr_ket`: the horizontal transfers (e0| -> (ij| and
         |f0) -> |kl), applied once per contracted quartet;
-  * the instantiation of the kernel template of csrc/jk_kernels.cuh for
+  * the instantiation of the kernel templates of csrc/jk_kernels.cuh for
     that class, and a host launcher registered in a table.
 
 The arithmetic follows the reference's Rys formulation (roots t^2, c0x, cpx,
@@ -139,38 +141,46 @@ class Emitter:
         return '\n'.join(self.lines)
 
 
+def _mul(a, b):
+    if a == '1':
+        return b
+    if b == '1':
+        return a
+    return f'{a} * {b}'
+
+
+def _fma(coef, g, rest):
+    """coef * g + rest, with g possibly the literal 1."""
+    if g == '1':
+        return f'({coef} + {rest})'
+    return f'fma({coef}, {g}, {rest})'
+
+
+def _scaled(n, name):
+    return name if n == 1 else f'T({n}) * {name}'
+
+
 def gen_vrr(em, cls, d, zero_one):
     """Emit G_d[e][f] for e <= lij, f <= lkl; returns dict (e, f) -> expr.
     zero_one: the value of G_d[0][0] ('1' for x and y, 'wz' for z)."""
     lij, lkl = cls.lij, cls.lkl
-    g = {}
-    g[(0, 0)] = zero_one
-
-    def mul(a, b):
-        if a == '1':
-            return b
-        if b == '1':
-            return a
-        return f'{a} * {b}'
-
+    g = {(0, 0): zero_one}
     for e in range(lij):
         name = f'g{d}_{e + 1}_0'
-        t = mul(f'c0{d}', g[(e, 0)])
+        t = _mul(f'c0{d}', g[(e, 0)])
         if e > 0:
-            em(f'const double {name} = fma({e}.0 * b10, {g[(e - 1, 0)]}, {t});')
-        else:
-            em(f'const double {name} = {t};')
+            t = _fma(_scaled(e, 'b10'), g[(e - 1, 0)], t)
+        em(f'const T {name} = {t};')
         g[(e + 1, 0)] = name
     for f in range(lkl):
         for e in range(lij + 1):
             name = f'g{d}_{e}_{f + 1}'
-            terms = mul(f'cp{d}', g[(e, f)])
-            expr = terms
+            expr = _mul(f'cp{d}', g[(e, f)])
             if f > 0:
-                expr = f'fma({f}.0 * b01, {g[(e, f - 1)]}, {expr})'
+                expr = _fma(_scaled(f, 'b01'), g[(e, f - 1)], expr)
             if e > 0:
-                expr = f'fma({e}.0 * b00, {g[(e - 1, f)]}, {expr})'
-            em(f'const double {name} = {expr};')
+                expr = _fma(_scaled(e, 'b00'), g[(e - 1, f)], expr)
+            em(f'const T {name} = {expr};')
             g[(e, f + 1)] = name
     return g
 
@@ -204,7 +214,7 @@ def gen_root_acc(cls):
             elif uses[key] > 1:
                 if key not in named:
                     nm = f'xy_{key[0]}{key[1]}{key[2]}{key[3]}'
-                    em(f'const double {nm} = {a} * {b};')
+                    em(f'const T {nm} = {a} * {b};')
                     named[key] = nm
                 xy = named[key]
             else:
@@ -258,11 +268,11 @@ def gen_hrr(la, lb, prefix, vec):
         t1 = val(L + 1, ap, k - 1, bm)
         t2 = val(L, a, k - 1, bm)
         name = f'{prefix}{k}_{L}_{cidx(L, a)}_{cidx(k, b)}'
-        em(f'const double {name} = fma({vec}{"xyz"[d]}, {t2}, {t1});')
+        em(f'const T {name} = fma({vec}{"xyz"[d]}, {t2}, {t1});')
         memo[key] = name
         return name
 
-    na, nb = ncart(la), ncart(lb)
+    nb = ncart(lb)
     outs = []
     for ia, a in enumerate(comps(la)):
         for ib, b in enumerate(comps(lb)):
@@ -273,7 +283,8 @@ def gen_hrr(la, lb, prefix, vec):
 
 
 def gen_class_header(cls):
-    E, F = cls.eset(), cls.fset()
+    E = cls.eset()
+    tpl = 'template <class T> __device__ static __forceinline__ void'
     lines = [f'struct Cls_{cls.tag} {{',
              f'    static constexpr int LI = {cls.li}, LJ = {cls.lj}, '
              f'LK = {cls.lk}, LL = {cls.ll};',
@@ -299,16 +310,14 @@ def gen_class_header(cls):
         lines.append(f'    __device__ static __forceinline__ int ez(int e) '
                      f'{{ constexpr int t[NE] = {{{ez}}}; return t[e]; }}')
         for p, (f0, f1) in enumerate(parts):
-            lines.append(f'    __device__ static __forceinline__ void row_acc_{p}('
-                         'const double *gx, const double *gy, const double *gz, '
-                         'double *acc) {')
+            lines.append(f'    {tpl} row_acc_{p}('
+                         'const T *gx, const T *gy, const T *gz, T *acc) {')
             lines.append(gen_row_acc(cls, f0, f1))
             lines.append('    }')
-        lines.append('    template <int P> __device__ static __forceinline__ void '
-                     'row_acc(const double *gx, const double *gy, const double *gz, '
-                     'double *acc) {')
+        lines.append('    template <int P, class T> __device__ static __forceinline__ void '
+                     'row_acc(const T *gx, const T *gy, const T *gz, T *acc) {')
         for p in range(len(parts)):
-            lines.append(f'        if (P == {p}) row_acc_{p}(gx, gy, gz, acc);')
+            lines.append(f'        if (P == {p}) row_acc_{p}<T>(gx, gy, gz, acc);')
         lines.append('    }')
         lines.append('    template <int P> __device__ static constexpr int fbegin() {')
         lines.append('        return ' + ' '.join(f'P == {p} ? {f0} :' for p, (f0, _) in enumerate(parts)) + ' 0;')
@@ -318,18 +327,15 @@ def gen_class_header(cls):
         lines.append('    }')
     else:
         lines.append('    static constexpr int TEAM_LANES = 1, NWF = 1, TEAM = 1, FPART = NF;')
-        lines.append('    __device__ static __forceinline__ void root_acc('
-                     'double c0x, double c0y, double c0z, double cpx, double cpy, '
-                     'double cpz, double b00, double b10, double b01, double wz, '
-                     'double *acc) {')
+        lines.append(f'    {tpl} root_acc('
+                     'T c0x, T c0y, T c0z, T cpx, T cpy, T cpz, T b00, T b10, T b01, '
+                     'T wz, T *acc) {')
         lines.append(gen_root_acc(cls))
         lines.append('    }')
-    lines.append('    __device__ static __forceinline__ void hrr_bra(const double *in, '
-                 'double *out, double ABx, double ABy, double ABz) {')
+    lines.append(f'    {tpl} hrr_bra(const T *in, T *out, T ABx, T ABy, T ABz) {{')
     lines.append(gen_hrr(cls.li, cls.lj, 'hb', 'AB'))
     lines.append('    }')
-    lines.append('    __device__ static __forceinline__ void hrr_ket(const double *in, '
-                 'double *out, double CDx, double CDy, double CDz) {')
+    lines.append(f'    {tpl} hrr_ket(const T *in, T *out, T CDx, T CDy, T CDz) {{')
     lines.append(gen_hrr(cls.lk, cls.ll, 'hk', 'CD'))
     lines.append('    }')
     lines.append('};')

@@ -42,10 +42,14 @@ import numpy as np
 LD = np.longdouble
 
 NMAX = 7            # up to (ff|ff): floor(12/2) + 1 roots
-H = 2.0             # interval width of the piecewise Chebyshev fit
+# Interval layout of the piecewise Chebyshev fit: (start, end, width) per
+# segment.  The roots vary fastest at small x, so the intervals are narrow
+# there; degree 9 keeps every root and weight within ~1e-14 relative for
+# n <= 7 (10 coefficients: five 16-byte loads per row in the kernels).
+SEGMENTS = ((0.0, 20.0, 0.5), (20.0, 40.0, 1.0), (40.0, 100.0, 2.0))
 XMAX = 100.0        # tables cover [0, XMAX); the Hermite limit is used above
-NINT = int(XMAX / H)
-DEGREE = 13         # Chebyshev degree per interval (DEGREE + 1 coefficients)
+NINT = sum(int(round((b - a) / h)) for a, b, h in SEGMENTS)
+DEGREE = 9          # Chebyshev degree per interval (DEGREE + 1 coefficients)
 DEGREE_F32 = 7      # degree of the single-precision table (mixed precision)
 
 
@@ -201,24 +205,84 @@ def _cheb_coeffs(f_vals, deg):
     return c
 
 
+def intervals():
+    """[(x_left, width)] of every interval, segment by segment."""
+    out = []
+    for a, b, h in SEGMENTS:
+        n = int(round((b - a) / h))
+        out += [(a + i * h, h) for i in range(n)]
+    return out
+
+
+def locate(x):
+    """(interval index, local variable s in [-1, 1]) as the kernels compute
+    them: segment by comparison, floor through the 1.5*2^52 rounding trick."""
+    it0 = 0
+    for a, b, h in SEGMENTS:
+        if x < b:
+            v = (x - a) / h
+            k = int(np.floor(v))
+            k = min(k, int(round((b - a) / h)) - 1)
+            return it0 + k, 2.0 * (v - k) - 1.0
+        it0 += int(round((b - a) / h))
+    raise ValueError(x)
+
+
 def fit_tables(deg: int = DEGREE, nmax: int = NMAX):
     """coef[n-1] has shape (NINT, 2n, deg+1): rows 0..n-1 are the roots,
-    rows n..2n-1 the weights, for the interval it = floor(x / H) and the
-    local variable s = (x - it*H) * (2/H) - 1."""
+    rows n..2n-1 the weights, on the intervals of SEGMENTS; the local
+    variable of interval [a, a + h) is s = 2 (x - a)/h - 1."""
     m = deg + 1
     k = np.arange(m, dtype=LD)
     cheb_pts = np.cos(np.pi * (k + LD(0.5)) / m)
     out = []
+    ivs = intervals()
     for n in range(1, nmax + 1):
-        tab = np.zeros((NINT, 2 * n, m), dtype=LD)
-        for it in range(NINT):
-            xs = it * LD(H) + (cheb_pts + 1) * LD(H) / 2
+        tab = np.zeros((len(ivs), 2 * n, m), dtype=LD)
+        for it, (a, h) in enumerate(ivs):
+            xs = LD(a) + (cheb_pts + 1) * LD(h) / 2
             vals = np.array([np.concatenate(rys_exact(n, float(xv)))
                              for xv in xs])        # (m, 2n)
             for row in range(2 * n):
                 tab[it, row] = _cheb_coeffs(vals[:, row], deg)
         out.append(tab)
     return out
+
+
+def cheb_to_monomial(c):
+    """sum_k c_k T_k(s) -> sum_k a_k s^k (long double)."""
+    n = len(c)
+    T = [np.zeros(n, dtype=LD) for _ in range(n)]
+    T[0][0] = 1
+    if n > 1:
+        T[1][1] = 1
+    for k in range(2, n):
+        T[k][1:] += 2 * T[k - 1][:-1]
+        T[k] -= T[k - 2]
+    a = np.zeros(n, dtype=LD)
+    for k in range(n):
+        a += c[k] * T[k]
+    return a
+
+
+def monomial(tab):
+    """Table of Chebyshev rows -> table of monomial rows, same shape."""
+    out = np.empty_like(tab)
+    for idx in np.ndindex(tab.shape[:-1]):
+        out[idx] = cheb_to_monomial(tab[idx])
+    return out
+
+
+def estrin(a, s):
+    """sum_k a_k s^k the way the kernels evaluate it (even degree count)."""
+    a = np.asarray(a, dtype=np.float64)
+    s = np.float64(s)
+    p = [a[k] + a[k + 1] * s for k in range(0, len(a), 2)]
+    s2 = s * s
+    while len(p) > 1:
+        q = [p[k] + (p[k + 1] * s2 if k + 1 < len(p) else 0.0) for k in range(0, len(p), 2)]
+        p, s2 = q, s2 * s2
+    return p[0]
 
 
 def clenshaw(c, s):
@@ -235,8 +299,7 @@ def eval_table(tabs, n, x):
     if x >= XMAX:
         r, w = rys_asymptotic(n, x)
         return r.astype(np.float64), w.astype(np.float64)
-    it = int(x / H)
-    s = (x - it * H) * (2.0 / H) - 1.0
+    it, s = locate(x)
     c = tabs[n - 1][it].astype(np.float64)
     vals = np.array([clenshaw(c[row], np.float64(s)) for row in range(2 * n)])
     return vals[:n], vals[n:]
@@ -272,9 +335,15 @@ def write_include(outdir: str) -> None:
         '// Generated by electrolites_b200/codegen/rys_table.py -- do not edit.',
         '#pragma once',
         f'#define RYS_NMAX {NMAX}',
-        f'#define RYS_H {H!r}',
-        f'#define RYS_INV_H {1.0 / H!r}',
         f'#define RYS_XMAX {XMAX!r}',
+        # segment boundaries, inverse widths and first interval of each
+        f'#define RYS_SEG1 {SEGMENTS[1][0]!r}',
+        f'#define RYS_SEG2 {SEGMENTS[2][0]!r}',
+        f'#define RYS_IH0 {1.0 / SEGMENTS[0][2]!r}',
+        f'#define RYS_IH1 {1.0 / SEGMENTS[1][2]!r}',
+        f'#define RYS_IH2 {1.0 / SEGMENTS[2][2]!r}',
+        f'#define RYS_IT1 {int(round((SEGMENTS[0][1] - SEGMENTS[0][0]) / SEGMENTS[0][2]))}',
+        f'#define RYS_IT2 {int(round((SEGMENTS[0][1] - SEGMENTS[0][0]) / SEGMENTS[0][2])) + int(round((SEGMENTS[1][1] - SEGMENTS[1][0]) / SEGMENTS[1][2]))}',
         f'#define RYS_NINT {NINT}',
         f'#define RYS_DEGREE {DEGREE}',
         f'#define RYS_DEGREE_F32 {DEGREE_F32}',
@@ -288,6 +357,10 @@ def write_include(outdir: str) -> None:
     lines = ['// Generated by electrolites_b200/codegen/rys_table.py -- do not edit.',
              '// Piecewise Chebyshev fits of the Rys roots (t^2) and weights.',
              '#pragma once']
+    # the kernels evaluate each row as a polynomial in s (Estrin's scheme),
+    # so the Chebyshev series are converted to monomial coefficients here
+    tabs = [monomial(t) for t in tabs]
+    tabs32 = [monomial(t) for t in tabs32]
     flat = np.concatenate([t.astype(np.float64).ravel() for t in tabs])
     lines.append('static const double rys_table_host[RYS_TABLE_SIZE] = {')
     for i in range(0, len(flat), 4):

@@ -16,6 +16,8 @@
 #include "generated/class_table.inc"
 #include "generated/rys_table_data.inc"
 
+#include <cub/cub.cuh>
+
 #define NPAIR_CLASSES 10          // (la, lb), la >= lb, l <= 3
 #define PLAN_DM_MARGIN 13.815511  // log(1e6): pairs kept for |D| up to 1e6
 
@@ -69,9 +71,19 @@ struct jk_plan {
     float *d_rys32 = nullptr;
     int *d_sh_ao = nullptr, *d_sh_nf = nullptr;
     int *d_counters = nullptr;
+    int *d_chunk = nullptr;         // task size per class of the last build
     unsigned long long *d_nq = nullptr;
     int *d_error = nullptr;
     float *d_dm_max = nullptr;
+    // ket sub-lists (equal primitive-pair count) per pair class
+    std::vector<int2> subs;
+    int sub_off[NPAIR_CLASSES + 1] = {0};
+    int2 *d_subs = nullptr;
+    // task rows of one class launch: candidates, chunks, prefix of chunks
+    int *d_rows = nullptr;
+    long long max_rows = 0;
+    void *d_cub = nullptr;
+    size_t cub_bytes = 0;
     // workspace
     char *d_ws = nullptr;
     size_t ws_size = 0;
@@ -111,6 +123,10 @@ static void free_plan(jk_plan *p)
     cudaFree(p->d_dm_max);
     cudaFree(p->d_ws);
     cudaFree(p->d_io);
+    cudaFree(p->d_subs);
+    cudaFree(p->d_rows);
+    cudaFree(p->d_chunk);
+    cudaFree(p->d_cub);
 }
 
 template <class T>
@@ -201,7 +217,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     float *d_q = nullptr;
     CK(upload(&d_rec, rec));
     CK(upload(&d_cand, cand));
-    CK(cudaMalloc(&p->d_prim, std::max<size_t>(1, rec.size()) * 8 * sizeof(double)));
+    CK(cudaMalloc(&p->d_prim, std::max<size_t>(1, rec.size()) * JK_PRIM_STRIDE * sizeof(double)));
     CK(cudaMalloc(&d_q, std::max<size_t>(1, cand.size()) * sizeof(float)));
 
     std::vector<double> rys_host(RYS_TOTAL);
@@ -254,8 +270,18 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     std::vector<PairRec> recs;
     for (int k = 0; k < NPAIR_CLASSES; ++k) {
         auto &v = byclass[k];
-        std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return q[a] > q[b]; });
+        // primitive-pair count first (sub-lists of equal loop bounds), then q
+        std::stable_sort(v.begin(), v.end(), [&](int a, int b) {
+            if (cand[a].w != cand[b].w) return cand[a].w > cand[b].w;
+            return q[a] > q[b];
+        });
         p->pc_off[k] = (int)recs.size();
+        p->sub_off[k] = (int)p->subs.size();
+        for (size_t t = 0; t < v.size(); ++t) {
+            if (t == 0 || cand[v[t]].w != cand[v[t - 1]].w)
+                p->subs.push_back(make_int2((int)t, (int)t));
+            p->subs.back().y = (int)t + 1;
+        }
         int mp = 0;
         for (int c : v) {
             const int i = cand[c].x, j = cand[c].y;
@@ -277,6 +303,22 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
         p->pc_maxprim[k] = mp;
     }
     p->pc_off[NPAIR_CLASSES] = (int)recs.size();
+    p->sub_off[NPAIR_CLASSES] = (int)p->subs.size();
+    CK(upload(&p->d_subs, p->subs));
+    // task rows: the largest (bra class pairs) x (ket class sub-lists)
+    long long max_rows = 1;
+    for (int A = 0; A < NPAIR_CLASSES; ++A)
+        for (int B = 0; B <= A; ++B)
+            max_rows = std::max<long long>(
+                max_rows, (long long)(p->pc_off[A + 1] - p->pc_off[A]) *
+                              (p->sub_off[B + 1] - p->sub_off[B]));
+    if (max_rows > (1ll << 31) - 1) return fail(JK_ERR_ARG, "molecule too large (task rows)");
+    CK(cudaMalloc(&p->d_rows, 4 * (size_t)max_rows * sizeof(int)));
+    CK(cudaMalloc(&p->d_chunk, JK_NCLASSES * sizeof(int)));
+    p->max_rows = max_rows;
+    p->cub_bytes = 0;
+    CK(cub::DeviceScan::InclusiveSum(nullptr, p->cub_bytes, p->d_rows, p->d_rows, (int)max_rows));
+    CK(cudaMalloc(&p->d_cub, std::max<size_t>(16, p->cub_bytes)));
     p->npairs = (long long)recs.size();
     CK(upload(&p->d_pairs, recs));
 
@@ -285,10 +327,10 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     CK(upload(&p->d_sh_ao, p->sh_ao));
     CK(upload(&p->d_sh_nf, nf));
     CK(cudaMalloc(&p->d_counters, JK_NCLASSES * sizeof(int)));
-    CK(cudaMalloc(&p->d_nq, 2 * JK_NCLASSES * sizeof(unsigned long long)));
+    CK(cudaMalloc(&p->d_nq, 3 * JK_NCLASSES * sizeof(unsigned long long)));
     CK(cudaMalloc(&p->d_error, sizeof(int)));
     CK(cudaMemset(p->d_error, 0, sizeof(int)));
-    CK(cudaMemset(p->d_nq, 0, 2 * JK_NCLASSES * sizeof(unsigned long long)));
+    CK(cudaMemset(p->d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long)));
     CK(cudaMalloc(&p->d_dm_max, sizeof(float)));
     CK(cudaDeviceSynchronize());
     return JK_OK;
@@ -349,7 +391,7 @@ static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int wit
     if (n_dm <= 0 || !dm) return fail(JK_ERR_ARG, "jk_build: no densities");
     if (hermi < 0 || hermi > 2) return fail(JK_ERR_ARG, "jk_build: hermi must be 0, 1 or 2");
     if ((with_j && !vj) || (with_k && !vk)) return fail(JK_ERR_ARG, "jk_build: output is NULL");
-    (void)mixed_threshold;
+    const float log_mixed = mixed_threshold > 0 ? (float)std::log(mixed_threshold) : -INFINITY;
     const int nao = p->nao;
     const size_t nao2 = (size_t)nao * nao;
     const int n_k = with_k ? (hermi == 0 ? 2 * n_dm : n_dm) : 0;
@@ -410,7 +452,7 @@ static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int wit
         p->launches += 3;
     }
     CK(cudaMemsetAsync(p->d_counters, 0, JK_NCLASSES * sizeof(int), st));
-    CK(cudaMemsetAsync(p->d_nq, 0, 2 * JK_NCLASSES * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(p->d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
 
     if (n_j || n_k) {
         LaunchCfg cfg;
@@ -418,6 +460,8 @@ static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int wit
         cfg.num_sms = p->num_sms;
         cfg.blocks_per_sm = 0;
         cfg.mixed = 0;
+        char launch_msg[256] = {0};
+        cfg.msg = launch_msg;
         for (int c = 0; c < JK_NCLASSES; ++c) {
             const ClassEntry &ce = jk_class_table[c];
             const int A = ce.bra_class, B = ce.ket_class;
@@ -448,14 +492,38 @@ static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int wit
             a.Kh = Kh;
             a.Jh = Jh;
             a.counter = p->d_counters + c;
+            a.sub = p->d_subs + p->sub_off[B];
+            a.nsub = p->sub_off[B + 1] - p->sub_off[B];
+            a.chunk = p->d_chunk + c;
+            a.row_ncand = p->d_rows;
+            int *chunks = p->d_rows + p->max_rows;
+            int *prefix = p->d_rows + 2 * p->max_rows;
+            int *cand_prefix = p->d_rows + 3 * p->max_rows;
+            a.row_prefix = prefix;
+            const int rows = nbra * a.nsub;
             a.nquartets = p->d_nq + c;
             a.nprimq = p->d_nq + JK_NCLASSES + c;
-            a.mixed_log_thr = -INFINITY;
+            a.mixed_log_thr = log_mixed;
+            a.nquartets32 = p->d_nq + 2 * JK_NCLASSES + c;
             a.error = p->d_error;
             if (p->timing) CK(cudaEventRecord(p->ev[2 * c], st));
+            // task list: candidates per row, a chunk size giving ~16 tasks per
+            // SM, chunks per row, prefix sum of chunks
+            task_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(a);
+            CK(cudaGetLastError());
+            size_t tmp_bytes = p->cub_bytes;
+            CK(cub::DeviceScan::InclusiveSum(p->d_cub, tmp_bytes, p->d_rows, cand_prefix, rows, st));
+            const int lo = ce.form == 0 ? 128 : 32, hi = ce.form == 0 ? 4096 : 1024;
+            const int target = (ce.form == 0 ? 64 : 16) * p->num_sms;
+            task_chunks_kernel<<<(rows + 255) / 256, 256, 0, st>>>(
+                p->d_rows, cand_prefix, rows, target, lo, hi, p->d_chunk + c, chunks);
+            CK(cudaGetLastError());
+            tmp_bytes = p->cub_bytes;
+            CK(cub::DeviceScan::InclusiveSum(p->d_cub, tmp_bytes, chunks, prefix, rows, st));
+            p->launches += 4;
             int rc = ce.launch(a, cfg);
             if (rc != 0)
-                return fail(JK_ERR_CUDA, std::string("class kernel launch failed: ") +
+                return fail(JK_ERR_CUDA, std::string("class kernel launch failed: ") + launch_msg + " " +
                                              cudaGetErrorString((cudaError_t)rc));
             if (p->timing) {
                 CK(cudaEventRecord(p->ev[2 * c + 1], st));
@@ -544,19 +612,21 @@ extern "C" int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int
 }
 
 extern "C" int jk_last_counts(jk_plan *plan, unsigned long long *quartets,
-                              unsigned long long *prim_quartets, int ncounts, int *nclasses)
+                              unsigned long long *prim_quartets,
+                              unsigned long long *quartets_f32, int ncounts, int *nclasses)
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_last_counts: plan is NULL");
     if (nclasses) *nclasses = JK_NCLASSES;
-    if (!quartets && !prim_quartets) return JK_OK;
+    if (!quartets && !prim_quartets && !quartets_f32) return JK_OK;
     DeviceGuard g(plan->device);
     CK(cudaStreamSynchronize(plan->last_stream));
-    std::vector<unsigned long long> h(2 * JK_NCLASSES);
-    CK(cudaMemcpy(h.data(), plan->d_nq, 2 * JK_NCLASSES * sizeof(unsigned long long),
+    std::vector<unsigned long long> h(3 * JK_NCLASSES);
+    CK(cudaMemcpy(h.data(), plan->d_nq, 3 * JK_NCLASSES * sizeof(unsigned long long),
                   cudaMemcpyDeviceToHost));
     for (int k = 0; k < ncounts && k < JK_NCLASSES; ++k) {
         if (quartets) quartets[k] = h[k];
         if (prim_quartets) prim_quartets[k] = h[JK_NCLASSES + k];
+        if (quartets_f32) quartets_f32[k] = h[2 * JK_NCLASSES + k];
     }
     return JK_OK;
 }

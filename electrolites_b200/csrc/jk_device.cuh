@@ -16,7 +16,16 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#define JK_PI_FAC 34.986836655249725   // 2 pi^(5/2)
+#define JK_PI_FAC 34.986836655249725        // 2 pi^(5/2)
+#define JK_SQRT_PI_FAC 5.914967172795612    // sqrt(2 pi^(5/2))
+
+// primitive-pair record: JK_PRIM_STRIDE doubles, fields at these offsets
+#define JK_PRIM_STRIDE 10
+#define PR_A 0      // a_ij
+#define PR_HIA 1    // 0.5 / a_ij
+#define PR_KP 2     // sqrt(2 pi^5/2) K_ij / a_ij
+#define PR_PX 3     // P (3)
+#define PR_PAX 6    // P - A (3)
 
 struct PairRec {
     int ish, jsh;        // shells; ish carries the higher angular momentum
@@ -50,9 +59,16 @@ struct ClassArgs {
     int n_j;
     double *Kh;              // half-K accumulators (n_k, nao, nao)
     double *Jh;              // half-J accumulators (n_j, nao, nao)
-    int *counter;            // work counter for the persistent grid
+    int *counter;            // task counter for the persistent grid
+    // task decomposition: rows r = bra * nsub + sub-list
+    const int2 *sub;         // ket sub-lists [begin, end) within the ket class
+    int nsub;
+    const int *chunk;        // kets per task (device scalar, set per launch)
+    const int *row_ncand;    // candidate kets per row
+    const int *row_prefix;   // inclusive prefix sum of chunks per row
     unsigned long long *nquartets;  // quartets evaluated (statistics)
     unsigned long long *nprimq;     // primitive quartets evaluated
+    unsigned long long *nquartets32;  // quartets evaluated in FP32
     float mixed_log_thr;     // mixed precision: quartets whose screened
                              // bound is below this run in FP32 (-inf: off)
     int *error;              // device error flag
@@ -74,11 +90,55 @@ struct ClassArgs {
 #define RYS_TOTAL (RYS_TABLE_SIZE + 2 * RYS_NMAX * RYS_NMAX)
 #define RYS32_TOTAL (RYS_TABLE32_SIZE + 2 * RYS_NMAX * RYS_NMAX)
 
+// Interval index and local variable s in [-1, 1] of x < RYS_XMAX.  The
+// segment is picked by comparison and floor((x - x0)/h) by adding 1.5*2^52,
+// which leaves the rounded integer in the low mantissa bits: no
+// double-to-int conversion, which would run on the XU pipe that the rsqrt
+// of every primitive quartet already occupies.
+__device__ __forceinline__ void rys_locate(double x, int &it, double &s)
+{
+    const bool g1 = x >= RYS_SEG1, g2 = x >= RYS_SEG2;
+    const double x0 = g2 ? RYS_SEG2 : (g1 ? RYS_SEG1 : 0.0);
+    const double ih = g2 ? RYS_IH2 : (g1 ? RYS_IH1 : RYS_IH0);
+    const int it0 = g2 ? RYS_IT2 : (g1 ? RYS_IT1 : 0);
+    const double v = (x - x0) * ih;
+    const double y = (v - 0.5) + 6755399441055744.0;     // 1.5 * 2^52
+    const double fk = y - 6755399441055744.0;
+    it = it0 + __double2loint(y);
+    s = 2.0 * (v - fk) - 1.0;
+}
+
+__device__ __forceinline__ void rys_locate_f32(float x, int &it, float &s)
+{
+    const bool g1 = x >= (float)RYS_SEG1, g2 = x >= (float)RYS_SEG2;
+    const float x0 = g2 ? (float)RYS_SEG2 : (g1 ? (float)RYS_SEG1 : 0.0f);
+    const float ih = g2 ? (float)RYS_IH2 : (g1 ? (float)RYS_IH1 : (float)RYS_IH0);
+    const int it0 = g2 ? RYS_IT2 : (g1 ? RYS_IT1 : 0);
+    const float v = (x - x0) * ih;
+    const float y = (v - 0.5f) + 12582912.0f;             // 1.5 * 2^23
+    const float fk = y - 12582912.0f;
+    it = it0 + (__float_as_int(y) & 0x3fffff);
+    s = 2.0f * (v - fk) - 1.0f;
+}
+
+// One table row, sum_k c_k s^k with k < 10, by Estrin's scheme (depth 4).
+__device__ __forceinline__ double rys_poly10(const double2 *__restrict__ cr, double s,
+                                             double s2, double s4, double s8)
+{
+    const double2 c01 = __ldg(cr), c23 = __ldg(cr + 1), c45 = __ldg(cr + 2);
+    const double2 c67 = __ldg(cr + 3), c89 = __ldg(cr + 4);
+    const double p0 = fma(c01.y, s, c01.x), p1 = fma(c23.y, s, c23.x);
+    const double p2 = fma(c45.y, s, c45.x), p3 = fma(c67.y, s, c67.x);
+    const double p4 = fma(c89.y, s, c89.x);
+    return fma(p4, s8, fma(fma(p3, s2, p2), s4, fma(p1, s2, p0)));
+}
+
 template <int N>
 __device__ __forceinline__ void rys_roots(double x, const double *__restrict__ tab,
                                           double *__restrict__ r,
                                           double *__restrict__ w)
 {
+    static_assert(RYS_DEGREE == 9, "rys_poly10 evaluates degree 9");
     if (x >= RYS_XMAX) {
         double ix = rsqrt(x);
         double inv = ix * ix;
@@ -89,41 +149,27 @@ __device__ __forceinline__ void rys_roots(double x, const double *__restrict__ t
         }
         return;
     }
-    int it = (int)(x * RYS_INV_H);
-    double s = fma(x - it * RYS_H, 2.0 * RYS_INV_H, -1.0);
-    double s2 = s + s;
-    const double *c = tab + rys_offset<N>() + it * (2 * N * (RYS_DEGREE + 1));
+    int it;
+    double s;
+    rys_locate(x, it, s);
+    const double s2 = s * s, s4 = s2 * s2, s8 = s4 * s4;
+    const double2 *c = reinterpret_cast<const double2 *>(
+        tab + rys_offset<N>() + it * (2 * N * (RYS_DEGREE + 1)));
 #pragma unroll
     for (int row = 0; row < 2 * N; ++row) {
-        const double2 *cr = reinterpret_cast<const double2 *>(c + row * (RYS_DEGREE + 1));
-        // Clenshaw: b_k = c_k + 2 s b_{k+1} - b_{k+2}
-        double b1 = 0., b2 = 0.;
-#pragma unroll
-        for (int k = (RYS_DEGREE + 1) / 2 - 1; k >= 1; --k) {
-            double2 cc = __ldg(cr + k);
-            double t = fma(s2, b1, cc.y - b2);
-            b2 = b1;
-            b1 = t;
-            t = fma(s2, b1, cc.x - b2);
-            b2 = b1;
-            b1 = t;
-        }
-        double2 c0 = __ldg(cr);
-        double t = fma(s2, b1, c0.y - b2);
-        b2 = b1;
-        b1 = t;
-        double v = fma(s, b1, c0.x - b2);
+        const double v = rys_poly10(c + row * (RYS_DEGREE + 1) / 2, s, s2, s4, s8);
         if (row < N) r[row] = v; else w[row - N] = v;
     }
 }
 
-// Single-precision variant for the mixed-precision form: a lower-degree
-// table, FP32 Clenshaw.  Accuracy ~1e-7 relative.
+// Single-precision variant for the mixed-precision form: a degree-7 table on
+// the same intervals, FP32 arithmetic.  Accuracy ~1e-7 relative.
 template <int N>
 __device__ __forceinline__ void rys_roots_f32(float x, const float *__restrict__ tab,
                                               float *__restrict__ r,
                                               float *__restrict__ w)
 {
+    static_assert(RYS_DEGREE_F32 == 7, "degree-7 single-precision table");
     if (x >= (float)RYS_XMAX) {
         float ix = rsqrtf(x);
         float inv = ix * ix;
@@ -134,23 +180,18 @@ __device__ __forceinline__ void rys_roots_f32(float x, const float *__restrict__
         }
         return;
     }
-    int it = (int)(x * (float)RYS_INV_H);
-    float s = fmaf(x - it * (float)RYS_H, 2.0f * (float)RYS_INV_H, -1.0f);
-    float s2 = s + s;
-    const float *c = tab + rys32_offset<N>() + it * (2 * N * (RYS_DEGREE_F32 + 1));
+    int it;
+    float s;
+    rys_locate_f32(x, it, s);
+    const float s2 = s * s, s4 = s2 * s2;
+    const float4 *c = reinterpret_cast<const float4 *>(
+        tab + rys32_offset<N>() + it * (2 * N * (RYS_DEGREE_F32 + 1)));
 #pragma unroll
     for (int row = 0; row < 2 * N; ++row) {
-        const float4 *cr = reinterpret_cast<const float4 *>(c + row * (RYS_DEGREE_F32 + 1));
-        float4 hi = __ldg(cr + 1), lo = __ldg(cr);
-        float cf[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-        float b1 = 0.f, b2 = 0.f;
-#pragma unroll
-        for (int k = RYS_DEGREE_F32; k >= 1; --k) {
-            float t = fmaf(s2, b1, cf[k] - b2);
-            b2 = b1;
-            b1 = t;
-        }
-        float v = fmaf(s, b1, cf[0] - b2);
+        const float4 lo = __ldg(c + 2 * row), hi = __ldg(c + 2 * row + 1);
+        const float p0 = fmaf(lo.y, s, lo.x), p1 = fmaf(lo.w, s, lo.z);
+        const float p2 = fmaf(hi.y, s, hi.x), p3 = fmaf(hi.w, s, hi.z);
+        const float v = fmaf(fmaf(p3, s2, p2), s4, fmaf(p1, s2, p0));
         if (row < N) r[row] = v; else w[row - N] = v;
     }
 }

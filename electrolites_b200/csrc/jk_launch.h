@@ -9,6 +9,7 @@ struct LaunchCfg {
     int num_sms;
     int blocks_per_sm;     // persistent grid: num_sms * blocks_per_sm blocks
     int mixed;             // 1: mixed-precision instantiation
+    char *msg;             // 256 bytes: launch failure details
 };
 
 typedef int (*ClassLauncher)(const ClassArgs &, const LaunchCfg &);

@@ -14,7 +14,10 @@ struct ShellDev {
 
 #define JK_PRIM_EXP_CUTOFF 60.0   // primitive pairs with a_i a_j/a_ij |AB|^2 > 60 are dropped
 
-// One record per kept primitive pair: {a_ij, K_ij, P, P - A}.
+// One record per kept primitive pair (JK_PRIM_STRIDE doubles):
+// {a_ij, 0.5/a_ij, Kp_ij, P, P - A, 0} with Kp_ij = sqrt(2 pi^5/2) K_ij / a_ij,
+// so that the primitive-quartet prefactor 2 pi^5/2 K_ij K_kl /
+// (a_ij a_kl sqrt(a_ij + a_kl)) is Kp_ij Kp_kl / sqrt(a_ij + a_kl).
 __global__ void prim_pair_fill_kernel(const int4 *__restrict__ rec, long long nrec,
                                       const ShellDev *__restrict__ sh,
                                       const double *__restrict__ basis_data,
@@ -31,15 +34,17 @@ __global__ void prim_pair_fill_kernel(const int4 *__restrict__ rec, long long nr
     const double rr = abx * abx + aby * aby + abz * abz;
     const double kij = ci * cj * exp(-ai * aj / aij * rr);
     const double t = aj / aij;
-    double *o = prim + r * 8;
-    o[0] = aij;
-    o[1] = kij;
-    o[2] = A.x - t * abx;       // P = A + aj/aij (B - A)
-    o[3] = A.y - t * aby;
-    o[4] = A.z - t * abz;
-    o[5] = -t * abx;            // P - A
-    o[6] = -t * aby;
-    o[7] = -t * abz;
+    double *o = prim + r * JK_PRIM_STRIDE;
+    o[PR_A] = aij;
+    o[PR_HIA] = 0.5 / aij;
+    o[PR_KP] = JK_SQRT_PI_FAC * kij / aij;
+    o[PR_PX] = A.x - t * abx;       // P = A + aj/aij (B - A)
+    o[PR_PX + 1] = A.y - t * aby;
+    o[PR_PX + 2] = A.z - t * abz;
+    o[PR_PAX] = -t * abx;           // P - A
+    o[PR_PAX + 1] = -t * aby;
+    o[PR_PAX + 2] = -t * abz;
+    o[9] = 0.;
 }
 
 // ---------------------------------------------------------------------------
@@ -90,16 +95,17 @@ __global__ void schwarz_kernel(const int4 *__restrict__ pairs, int npairs,
     double G[7][7], Ib[4][4][7], I[3][4][4][4][4];
     double r[7], w[7];
     for (int kp = 0; kp < pr.w; ++kp) {
-        const double *K = prim + (size_t)(pr.z + kp) * 8;
-        const double akl = K[0];
+        const double *K = prim + (size_t)(pr.z + kp) * JK_PRIM_STRIDE;
+        const double akl = K[PR_A];
         for (int bp = 0; bp < pr.w; ++bp) {
-            const double *P = prim + (size_t)(pr.z + bp) * 8;
-            const double aij = P[0];
-            const double PQ[3] = {P[2] - K[2], P[3] - K[3], P[4] - K[4]};
+            const double *P = prim + (size_t)(pr.z + bp) * JK_PRIM_STRIDE;
+            const double aij = P[PR_A];
+            const double PQ[3] = {P[PR_PX] - K[PR_PX], P[PR_PX + 1] - K[PR_PX + 1],
+                                  P[PR_PX + 2] - K[PR_PX + 2]};
             const double s = aij + akl;
             const double rr = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
             const double x = aij * akl / s * rr;
-            const double pref = JK_PI_FAC * P[1] * K[1] / (aij * akl * sqrt(s));
+            const double pref = P[PR_KP] * K[PR_KP] / sqrt(s);
             rys_roots_rt(nroots, x, rys, r, w);
             for (int ir = 0; ir < nroots; ++ir) {
                 const double u = r[ir];
@@ -108,8 +114,8 @@ __global__ void schwarz_kernel(const int4 *__restrict__ pairs, int npairs,
                 const double b10 = 0.5 / aij * (1 - up);
                 const double b01 = 0.5 / akl * (1 - uq);
                 for (int d = 0; d < 3; ++d) {
-                    const double c0 = P[5 + d] - up * PQ[d];
-                    const double cp = K[5 + d] + uq * PQ[d];
+                    const double c0 = P[PR_PAX + d] - up * PQ[d];
+                    const double cp = K[PR_PAX + d] + uq * PQ[d];
                     G[0][0] = d == 2 ? w[ir] * pref : 1.0;
                     for (int e = 0; e < lij; ++e)
                         G[e + 1][0] = c0 * G[e][0] + (e ? e * b10 * G[e - 1][0] : 0.);
@@ -243,4 +249,42 @@ __global__ void transpose_kernel(const double *__restrict__ D, int nao, double *
         const int r = by + k, c = bx + threadIdx.x;
         if (r < nao && c < nao) o[(size_t)r * nao + c] = tile[threadIdx.x][k];
     }
+}
+
+// Rows of the task decomposition: one per (bra pair b, ket sub-list s),
+// r = b * nsub + s.  row_ncand[r] = kets of sub-list s (sorted by q) that can
+// pass the Schwarz test with the largest density element, limited to ket
+// index <= b within a diagonal class.
+__global__ void task_rows_kernel(const ClassArgs a)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nbra * a.nsub) return;
+    const int b = r / a.nsub, s = r - (r / a.nsub) * a.nsub;
+    const float cut = a.log_tol - a.bra[b].q - *a.dm_max;
+    int lo = a.sub[s].x, hi = a.sub[s].y;
+    if (a.same_class && hi > b + 1) hi = b + 1;
+    const int first = lo;
+    if (lo > hi) hi = lo;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a.ket[mid].q > cut) lo = mid + 1; else hi = mid;
+    }
+    const_cast<int *>(a.row_ncand)[r] = lo - first;
+}
+
+// Task size from the class's total candidate count (cand_prefix[rows-1]):
+// about `target` tasks, clamped to [lo, hi] kets and rounded to a warp; then
+// the chunk count of every row.
+__global__ void task_chunks_kernel(const int *__restrict__ ncand, const int *__restrict__ cand_prefix,
+                                   int rows, int target, int lo, int hi, int *__restrict__ chunk_out,
+                                   int *__restrict__ chunks)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = rows > 0 ? cand_prefix[rows - 1] : 0;
+    long long c = (total + target - 1) / target;
+    c = (c + 31) / 32 * 32;
+    if (c < lo) c = lo;
+    if (c > hi) c = hi;
+    if (r == 0) *chunk_out = (int)c;
+    if (r < rows) chunks[r] = (int)((ncand[r] + c - 1) / c);
 }

@@ -168,23 +168,24 @@ class VHFOpt:
         vj, _ = self.get_jk(dms, hermi, verbose, with_j=True, with_k=False)
         return vj
 
-    def class_counts(self):
+    def class_counts(self, with_f32=False):
         """{(li, lj, lk, ll): (quartets, primitive quartets)} evaluated by the
-        last build."""
+        last build; with_f32 appends the quartets evaluated in FP32."""
         L = _lib.lib()
         ncls = ctypes.c_int()
-        _lib.check(L.jk_last_counts(self.plan, None, None, 0, ctypes.byref(ncls)),
+        _lib.check(L.jk_last_counts(self.plan, None, None, None, 0, ctypes.byref(ncls)),
                    'jk_last_counts')
         q = (ctypes.c_ulonglong * ncls.value)()
         pq = (ctypes.c_ulonglong * ncls.value)()
-        _lib.check(L.jk_last_counts(self.plan, q, pq, ncls.value, ctypes.byref(ncls)),
+        q32 = (ctypes.c_ulonglong * ncls.value)()
+        _lib.check(L.jk_last_counts(self.plan, q, pq, q32, ncls.value, ctypes.byref(ncls)),
                    'jk_last_counts')
         out = {}
         for k in range(ncls.value):
             ls = [ctypes.c_int() for _ in range(5)]
             _lib.check(L.jk_class_info(k, *[ctypes.byref(x) for x in ls]), 'jk_class_info')
             key = tuple(x.value for x in ls[:4])
-            out[key] = (int(q[k]), int(pq[k]))
+            out[key] = (int(q[k]), int(pq[k])) + ((int(q32[k]),) if with_f32 else ())
         return out
 
     def set_timing(self, enable=True):

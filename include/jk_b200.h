@@ -93,13 +93,14 @@ int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi,
 int jk_sync(jk_plan *plan, void *stream);
 
 /*
- * Shell quartets and primitive quartets evaluated by the last build, per
- * angular-momentum class (index k of jk_class_info), and the number of
- * classes.  Either array may be NULL.  Synchronises the stream of the last
- * build.
+ * Shell quartets, primitive quartets and FP32-evaluated quartets of the
+ * last build, per angular-momentum class (index k of jk_class_info), and
+ * the number of classes.  Any array may be NULL.  Synchronises the stream
+ * of the last build.
  */
 int jk_last_counts(jk_plan *plan, unsigned long long *quartets,
-                   unsigned long long *prim_quartets, int ncounts,
+                   unsigned long long *prim_quartets,
+                   unsigned long long *quartets_f32, int ncounts,
                    int *nclasses);
 
 /* li, lj, lk, ll and the form (0 register, 1 team) of class k. */

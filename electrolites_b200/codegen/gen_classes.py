@@ -32,7 +32,7 @@ import os
 import sys
 from dataclasses import dataclass
 
-REG_MAX = 81          # largest (e0|f0) block kept in one thread's registers
+REG_MAX = 100         # largest (e0|f0) block kept in one thread's registers
 FPART_MAX = 40        # f-components per warp in the team form
 LMAX = 3
 

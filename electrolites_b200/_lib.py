@@ -18,7 +18,7 @@ JK_ERRORS = {1: 'invalid argument', 2: 'unsupported shell', 3: 'CUDA error',
 
 EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_build_host', 'jk_sync', 'jk_last_counts', 'jk_class_info',
-           'jk_set_timing', 'jk_last_class_ms', 'jk_fp64_peak',
+           'jk_set_timing', 'jk_last_class_ms', 'jk_fp64_peak', 'jk_build_noalloc',
            'jk_plan_q_cond', 'jk_last_error']
 
 _lib = None
@@ -47,6 +47,7 @@ def lib():
     L.jk_plan_info.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_longlong)]
     L.jk_build.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, vp]
     L.jk_build_host.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, vp]
+    L.jk_build_noalloc.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, vp]
     L.jk_sync.argtypes = [vp, vp]
     L.jk_last_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong),
                                  ctypes.POINTER(ctypes.c_ulonglong),

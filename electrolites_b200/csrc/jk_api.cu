@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -385,8 +386,11 @@ extern "C" int jk_plan_q_cond(const jk_plan *plan, float *q_host, int nbas)
 
 static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
+// ws_ext: when not NULL, the build's workspace is taken from this caller-owned
+// device buffer of ws_ext_size bytes instead of the plan's own allocation.
 static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int with_j, int with_k,
-                      double *vj, double *vk, double mixed_threshold, cudaStream_t st)
+                      double *vj, double *vk, double mixed_threshold, cudaStream_t st,
+                      char *ws_ext = nullptr, size_t ws_ext_size = 0)
 {
     if (n_dm <= 0 || !dm) return fail(JK_ERR_ARG, "jk_build: no densities");
     if (hermi < 0 || hermi > 2) return fail(JK_ERR_ARG, "jk_build: hermi must be 0, 1 or 2");
@@ -404,7 +408,15 @@ static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int wit
     const size_t o_dt = o_ds + align256((size_t)n_j * nao2 * 8);
     const size_t o_dc = o_dt + align256(need_t ? (size_t)n_dm * nao2 * 8 : 0);
     const size_t need = o_dc + align256((size_t)p->nbas * p->nbas * 4);
-    if (need > p->ws_size) {
+    char *ws = p->d_ws;
+    if (ws_ext) {
+        if (need > ws_ext_size)
+            return fail(JK_ERR_RANGE, "jk_build_noalloc: this build needs " + std::to_string(need) +
+                                          " bytes of scratch, the library's static scratch holds " +
+                                          std::to_string(ws_ext_size) +
+                                          " (use jk_build for larger molecules or more densities)");
+        ws = ws_ext;
+    } else if (need > p->ws_size) {
         CK(cudaStreamSynchronize(st));
         cudaFree(p->d_ws);
         p->d_ws = nullptr;
@@ -415,12 +427,13 @@ static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int wit
                                           " bytes of workspace");
         }
         p->ws_size = need;
+        ws = p->d_ws;
     }
-    double *Kh = (double *)(p->d_ws + o_kh);
-    double *Jh = (double *)(p->d_ws + o_jh);
-    double *dsJ = (double *)(p->d_ws + o_ds);
-    double *DT = (double *)(p->d_ws + o_dt);
-    float *dmc = (float *)(p->d_ws + o_dc);
+    double *Kh = (double *)(ws + o_kh);
+    double *Jh = (double *)(ws + o_jh);
+    double *dsJ = (double *)(ws + o_ds);
+    double *DT = (double *)(ws + o_dt);
+    float *dmc = (float *)(ws + o_dc);
     p->last_stream = st;
     p->launches = 0;
     if (p->timing) std::fill(p->ev_used.begin(), p->ev_used.end(), 0);
@@ -577,6 +590,49 @@ extern "C" int jk_sync(jk_plan *plan, void *stream)
         return fail(JK_ERR_DEVICE, "kernel error flag " + std::to_string(err));
     }
     return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free build.  Its scratch (the half-J/K accumulators, the
+// symmetrised and transposed densities and the density screening table)
+// lives in this fixed array, which every GPU that loads the library holds
+// until the process exits.  Host code must not pass the array's name to a
+// kernel: on the host it is only a stand-in, so its device address is looked
+// up with cudaGetSymbolAddress, once per device, with that device current.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[JK_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mutex;
+static void *g_noalloc_addr[JK_NOALLOC_MAX_DEVICES];
+
+static int noalloc_scratch(int device, char **out)
+{
+    if (device < 0 || device >= JK_NOALLOC_MAX_DEVICES)
+        return fail(JK_ERR_ARG, "jk_build_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[device]) {
+        void *ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(JK_ERR_CUDA, std::string("jk_build_noalloc: cudaGetSymbolAddress: ") +
+                                         cudaGetErrorString(e));
+        g_noalloc_addr[device] = ptr;
+    }
+    *out = (char *)g_noalloc_addr[device];
+    return JK_OK;
+}
+
+extern "C" int jk_build_noalloc(jk_plan *plan, const double *dm, int n_dm, int hermi, int with_j,
+                                int with_k, double *vj, double *vk, double mixed_threshold,
+                                void *stream)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_build_noalloc: plan is NULL");
+    DeviceGuard g(plan->device);
+    char *scratch = nullptr;
+    const int rc = noalloc_scratch(plan->device, &scratch);
+    if (rc) return rc;
+    return build_impl(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
+                      (cudaStream_t)stream, scratch, (size_t)JK_NOALLOC_SCRATCH_BYTES);
 }
 
 extern "C" int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi, int with_j,

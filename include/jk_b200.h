@@ -88,6 +88,36 @@ int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi,
                   int with_j, int with_k, double *vj_host, double *vk_host,
                   double mixed_threshold, void *stream);
 
+/*
+ * jk_build without any device allocation.  No counterpart in the reference:
+ * it exists for callers that cannot let a library call cudaMalloc -- an SCF
+ * driver that hands all device memory to its own caching pool (PyTorch,
+ * CuPy) and would fragment it or run out behind the pool's back, a
+ * latency-critical serving path where a cudaMalloc or cudaFree would
+ * synchronise the device, or a host that only allows memory it manages.
+ *
+ * The build's scratch (half-J/K accumulators, symmetrised and transposed
+ * densities, density screening table) comes from one fixed array of
+ * JK_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads
+ * the library keeps until the process exits.  A build whose scratch would
+ * not fit -- about n_k + 2 n_j density-sized double matrices plus
+ * nbas^2 floats, e.g. nao up to ~700 for two symmetric densities -- is
+ * rejected with JK_ERR_RANGE before anything is launched.  The plan must
+ * already exist (jk_plan_create allocates; create it at set-up).
+ *
+ * The first call on a device looks up the array's device address (with
+ * that device current); make that first call before any stream capture.
+ * Every call shares the one array and it keeps the previous call's
+ * contents (the accumulators are cleared at the start of each call), so
+ * calls whose work overlaps on the GPU -- different streams, or different
+ * plans on one device -- race with each other: serialise them.
+ */
+#define JK_NOALLOC_SCRATCH_BYTES (24u << 20)
+#define JK_NOALLOC_MAX_DEVICES 64
+int jk_build_noalloc(jk_plan *plan, const double *dm, int n_dm, int hermi,
+                     int with_j, int with_k, double *vj, double *vk,
+                     double mixed_threshold, void *stream);
+
 /* Wait for the plan's work on stream; returns JK_ERR_DEVICE if a kernel
  * raised its error flag (the flag is then cleared). */
 int jk_sync(jk_plan *plan, void *stream);

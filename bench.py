@@ -153,6 +153,103 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+BATCH_SEED = 20261206
+BATCH_MOLS = 512
+BATCH_MIXED = 1e-6
+
+
+def _timed(fn, steps, warmup, stream, flush):
+    """Device ms per call of fn(): CUDA events on `stream`, L2 flushed
+    (untimed) before each timed call."""
+    import torch
+    for _ in range(max(3, warmup)):
+        fn()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        fn()
+        e.record(stream)
+        e.synchronize()
+        total += s.elapsed_time(e)
+    return total / steps
+
+
+def run_batch(args, dev, stream, flush, peak_tflops):
+    """Uneven batch: 512 water clusters (n ~ U{1..24}, cube 3.1 n^(1/3) A,
+    6-31G*, 1-4 densities each, seed 20261206).  Times the plain FP64 form
+    as one build per molecule, and the batched form (one launch stream for
+    all molecules, replayed from a CUDA graph) in FP64 and mixed precision;
+    reports molecule-builds per second and the mixed form's largest J/K
+    energy error against the plain one."""
+    import torch
+
+    from electrolites_b200 import clusters, flop_model
+    from electrolites_b200.batch import JKBatch
+    from electrolites_b200.jk import VHFOpt
+    t0 = time.perf_counter()
+    items = clusters.uneven_batch(BATCH_MOLS, BATCH_SEED)
+    opts = [VHFOpt(m, TOL, device=dev.index).build() for m, _ in items]
+    dms = [torch.as_tensor(d, device=dev) for _, d in items]
+    setup_s = time.perf_counter() - t0
+    vj = [torch.empty_like(d) for d in dms]
+    vk = [torch.empty_like(d) for d in dms]
+    bj = [torch.empty_like(d) for d in dms]
+    bk = [torch.empty_like(d) for d in dms]
+    batch = JKBatch(dev.index)
+
+    def seq():
+        for o, d, j, k in zip(opts, dms, vj, vk):
+            o.build_jk_async(d, 1, True, True, j, k, 0.0, stream)
+
+    def bat(thr):
+        return lambda: batch.build_async(opts, dms, 1, True, True, bj, bk, thr, True, stream)
+
+    steps, warm = max(2, min(args.steps, 3)), args.warmup
+    ms_plain = _timed(seq, steps, warm, stream, flush)
+    for o in opts:
+        o.sync(stream)
+    ej = torch.stack([0.5 * (d * j).sum() for d, j in zip(dms, vj)])
+    ek = torch.stack([-0.25 * (d * k).sum() for d, k in zip(dms, vk)])
+    ms_b64 = _timed(bat(0.0), steps, warm, stream, flush)
+    batch.sync(stream)
+    counts = batch.class_counts()
+    err64 = max(float((torch.stack([0.5 * (d * j).sum() for d, j in zip(dms, bj)]) - ej).abs().max()),
+                float((torch.stack([-0.25 * (d * k).sum() for d, k in zip(dms, bk)]) - ek).abs().max()))
+    ms_mix = _timed(bat(BATCH_MIXED), steps, warm, stream, flush)
+    batch.sync(stream)
+    st = batch.stats()
+    c32 = batch.class_counts(with_f32=True)
+    errj = float((torch.stack([0.5 * (d * j).sum() for d, j in zip(dms, bj)]) - ej).abs().max())
+    errk = float((torch.stack([-0.25 * (d * k).sum() for d, k in zip(dms, bk)]) - ek).abs().max())
+    _, launches = batch.last_class_ms()
+    # algorithmic flops of the batch: the model per molecule needs per-molecule
+    # counts, so the class totals are used with the mean density count
+    n_dm = sum(d.shape[0] for d in dms)
+    flops = flop_model.build_flops(counts, n_dm / len(dms), n_dm / len(dms))
+    nq = sum(v[0] for v in counts.values())
+    nq32 = sum(v[2] for v in c32.values())
+    return {
+        'workload': f'batch{BATCH_MOLS}_631gs', 'molecules': BATCH_MOLS, 'densities': n_dm,
+        'nao_cart_mean': sum(o.nao for o in opts) / len(opts),
+        'nao_cart_max': max(o.nao for o in opts), 'setup_s': round(setup_s, 1),
+        'steps': steps, 'quartets': nq,
+        'plain_ms': ms_plain, 'plain_mol_builds_per_s': BATCH_MOLS * 1e3 / ms_plain,
+        'batched_fp64_ms': ms_b64, 'batched_fp64_mol_builds_per_s': BATCH_MOLS * 1e3 / ms_b64,
+        'batched_fp64_energy_err': err64,
+        'batched_mixed_ms': ms_mix, 'batched_mixed_mol_builds_per_s': BATCH_MOLS * 1e3 / ms_mix,
+        'mixed_threshold': BATCH_MIXED, 'mixed_fp32_quartet_frac': nq32 / max(1, nq),
+        'mixed_energy_err_j': errj, 'mixed_energy_err_k': errk,
+        'speedup_batched_fp64_vs_plain': ms_plain / ms_b64,
+        'speedup_batched_mixed_vs_plain': ms_plain / ms_mix,
+        'batched_fp64_tflops_model': flops / (ms_b64 * 1e-3) / 1e12,
+        'batched_fp64_peak_frac': flops / (ms_b64 * 1e-3) / 1e12 / peak_tflops,
+        'graph_replayed': st['graph_replayed'], 'launches_per_build': launches,
+    }
+
+
 def run_ours(args, rank, world):
     import ctypes
 
@@ -261,6 +358,10 @@ def run_ours(args, rank, world):
     # correctness guard on the timed output: symmetric, finite
     assert torch.isfinite(vj).all() and torch.isfinite(vk).all()
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batched = run_batch(args, dev, stream, flush, peak_tflops)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, thr_used, desc = cpu_sample(mol, dms_h, budget_s=args.cpu_budget)
@@ -295,6 +396,7 @@ def run_ours(args, rank, world):
             'gpu_launches': launches * args.steps,
             'clocks': clk,
             'cpu_baseline': cpu,
+            'batched': batched,
         }
         print(json.dumps(line), flush=True)
 
@@ -309,6 +411,8 @@ def main():
     ap.add_argument('--mixed', type=float, default=0.0)
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-batch', action='store_true',
+                    help='skip the uneven-batch comparison (plain vs batched vs mixed)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', 1))
     rank = int(os.environ.get('RANK', 0))

@@ -19,7 +19,10 @@ JK_ERRORS = {1: 'invalid argument', 2: 'unsupported shell', 3: 'CUDA error',
 EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_build_host', 'jk_sync', 'jk_last_counts', 'jk_class_info',
            'jk_set_timing', 'jk_last_class_ms', 'jk_fp64_peak', 'jk_build_noalloc',
-           'jk_plan_q_cond', 'jk_last_error']
+           'jk_plan_q_cond', 'jk_plan_memory', 'jk_plan_set_shard', 'jk_plan_set_tuning',
+           'jk_batch_create', 'jk_batch_destroy', 'jk_batch_build', 'jk_batch_sync',
+           'jk_batch_counts', 'jk_batch_set_timing', 'jk_batch_class_ms',
+           'jk_batch_set_tuning', 'jk_batch_stats', 'jk_last_error']
 
 _lib = None
 
@@ -57,6 +60,21 @@ def lib():
     L.jk_set_timing.argtypes = [vp, c_int]
     L.jk_last_class_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ip]
     L.jk_fp64_peak.argtypes = [c_int, ctypes.POINTER(ctypes.c_double)]
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    ullp = ctypes.POINTER(ctypes.c_ulonglong)
+    L.jk_plan_memory.argtypes = [vp, llp, llp]
+    L.jk_plan_set_shard.argtypes = [vp, c_int, c_int]
+    L.jk_plan_set_tuning.argtypes = [vp, c_int, c_int, c_int]
+    L.jk_batch_create.argtypes = [c_int, ctypes.POINTER(vp)]
+    L.jk_batch_destroy.argtypes = [vp]
+    L.jk_batch_build.argtypes = [vp, vp, c_int, vp, vp, c_int, c_int, c_int, vp, vp, c_double,
+                                 c_int, vp]
+    L.jk_batch_sync.argtypes = [vp, vp]
+    L.jk_batch_counts.argtypes = [vp, ullp, ullp, ullp, c_int, ip]
+    L.jk_batch_set_timing.argtypes = [vp, c_int]
+    L.jk_batch_class_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ip]
+    L.jk_batch_set_tuning.argtypes = [vp, c_int, c_int, c_int]
+    L.jk_batch_stats.argtypes = [vp, ip, ip, llp]
     L.jk_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:
         if name != 'jk_last_error':

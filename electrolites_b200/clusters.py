@@ -124,3 +124,35 @@ def uhf_pair(D: np.ndarray, seed: int, sigma_rel: float = 1e-3):
     p = rng.standard_normal(D.shape) * (sigma_rel * np.abs(da).max())
     p = (p + p.T) / math.sqrt(2)
     return np.stack([da, da + p])
+
+
+def density_stack(D: np.ndarray, n_dm: int, seed: int, sigma_rel: float = 1e-3):
+    """n_dm densities made like the UHF pair: D/2, then D/2 plus independent
+    seeded symmetric Gaussian perturbations (sigma_rel * max|D/2|)."""
+    if n_dm == 1:
+        return (0.5 * D)[None].copy()
+    rng = np.random.default_rng(seed)
+    da = 0.5 * D
+    out = [da]
+    for _ in range(n_dm - 1):
+        p = rng.standard_normal(D.shape) * (sigma_rel * np.abs(da).max())
+        out.append(da + (p + p.T) / math.sqrt(2))
+    return np.stack(out)
+
+
+def uneven_batch(n_mol: int, seed: int, n_min: int = 1, n_max: int = 24,
+                 bases=('6-31g*',), dm_min: int = 1, dm_max: int = 4):
+    """Seeded batch of uneven water clusters: per molecule n ~ U{n_min..n_max}
+    waters in a cube of edge 3.1 n^(1/3) A (2.7 A minimum O-O), a basis drawn
+    uniformly from `bases`, and 1..4 densities (density_stack of its atomic
+    density).  Returns [(mol, dms), ...]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_mol):
+        n = int(rng.integers(n_min, n_max + 1))
+        k = int(rng.integers(dm_min, dm_max + 1))
+        basis = bases[int(rng.integers(0, len(bases)))]
+        s = seed * 1000 + i
+        mol = water_mole(n, 3.1 * n ** (1.0 / 3.0), s, basis=basis)
+        out.append((mol, density_stack(atomic_density(mol, s), k, s + 1)))
+    return out

@@ -1,6 +1,17 @@
-// Plan construction, build driver and C ABI of the B200 J/K engine
+// Plan construction, build engine and C ABI of the B200 J/K engine
 // (declared in include/jk_b200.h).
+//
+// A build is a list of items, one per plan (molecule) with its densities and
+// outputs.  jk_build is a list of one; jk_batch_build is a list of hundreds.
+// Either way the build is the same stream of launches: one density pass over
+// all items (symmetrised / transposed densities), one screening-table pass,
+// then per angular-momentum class one persistent kernel over the task rows
+// of every item, and one J/K assembly pass.  Every per-item pointer and size
+// the kernels read comes from one descriptor blob uploaded per build (and
+// skipped when it is unchanged), so a batch's launch stream can be captured
+// once in a CUDA graph and replayed for new density values.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -37,6 +48,12 @@ static int fail(int code, const std::string &msg)
             return fail(JK_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
     } while (0)
 
+#define RC(call)                  \
+    do {                          \
+        const int r_ = (call);    \
+        if (r_ != JK_OK) return r_; \
+    } while (0)
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev)
@@ -50,54 +67,7 @@ struct DeviceGuard {
     }
 };
 
-struct jk_plan {
-    int device = 0;
-    int num_sms = 148;
-    int nbas_user = 0, nbas = 0, nao = 0;
-    bool expanded = false;          // a general contraction was split
-    std::vector<int> sh_l, sh_ao, sh_user;
-    double tol = 1e-13;
-    float log_tol = 0.f;
-    float q_max = -INFINITY, q_drop_max = -INFINITY;
-    long long npairs = 0;
-    int pc_off[NPAIR_CLASSES + 1] = {0};
-    int pc_maxprim[NPAIR_CLASSES] = {0};
-    std::vector<float> q_full;      // nbas x nbas (expanded numbering)
-    // device tables
-    ShellDev *d_shells = nullptr;
-    double *d_basis = nullptr;
-    double *d_prim = nullptr;
-    PairRec *d_pairs = nullptr;
-    double *d_rys = nullptr;
-    float *d_rys32 = nullptr;
-    int *d_sh_ao = nullptr, *d_sh_nf = nullptr;
-    int *d_counters = nullptr;
-    int *d_chunk = nullptr;         // task size per class of the last build
-    unsigned long long *d_nq = nullptr;
-    int *d_error = nullptr;
-    float *d_dm_max = nullptr;
-    // ket sub-lists (equal primitive-pair count) per pair class
-    std::vector<int2> subs;
-    int sub_off[NPAIR_CLASSES + 1] = {0};
-    int2 *d_subs = nullptr;
-    // task rows of one class launch: candidates, chunks, prefix of chunks
-    int *d_rows = nullptr;
-    long long max_rows = 0;
-    void *d_cub = nullptr;
-    size_t cub_bytes = 0;
-    // workspace
-    char *d_ws = nullptr;
-    size_t ws_size = 0;
-    double *d_io = nullptr;         // device buffers of jk_build_host
-    size_t io_size = 0;
-    cudaStream_t last_stream = nullptr;
-    // per-class timing and launch count of the last build
-    bool timing = false;
-    std::vector<cudaEvent_t> ev;    // 2 per class
-    std::vector<char> ev_used;
-    int launches = 0;
-};
-
+static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 static int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 static int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
 
@@ -108,37 +78,773 @@ static double common_fac(int l)
     return 1.0;
 }
 
+// the class units keep per-kernel launch state (shared-memory opt-in,
+// occupancy); builds from several host threads take turns there
+static std::mutex g_launch_mutex;
+
+// ---------------------------------------------------------------------------
+// Rys tables: one copy per device, shared by every plan, kept until exit
+// ---------------------------------------------------------------------------
+static std::mutex g_rys_mutex;
+static double *g_rys[JK_MAX_DEVICES];
+static float *g_rys32[JK_MAX_DEVICES];
+
+static int rys_tables(int device, const double **rys, const float **rys32)
+{
+    if (device < 0 || device >= JK_MAX_DEVICES) return fail(JK_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_rys_mutex);
+    if (!g_rys[device]) {
+        std::vector<double> h(RYS_TOTAL);
+        std::memcpy(h.data(), rys_table_host, sizeof(rys_table_host));
+        std::vector<float> h32(RYS32_TOTAL);
+        std::memcpy(h32.data(), rys_table32_host, sizeof(rys_table32_host));
+        for (int n = 0; n < RYS_NMAX; ++n)
+            for (int k = 0; k < RYS_NMAX; ++k) {
+                h[RYS_LARGEX_OFF + n * RYS_NMAX + k] = rys_largex_r_host[n][k];
+                h[RYS_LARGEX_OFF + RYS_NMAX * RYS_NMAX + n * RYS_NMAX + k] = rys_largex_w_host[n][k];
+                h32[RYS32_LARGEX_OFF + n * RYS_NMAX + k] = (float)rys_largex_r_host[n][k];
+                h32[RYS32_LARGEX_OFF + RYS_NMAX * RYS_NMAX + n * RYS_NMAX + k] =
+                    (float)rys_largex_w_host[n][k];
+            }
+        double *d = nullptr;
+        float *d32 = nullptr;
+        CK(cudaMalloc(&d, h.size() * sizeof(double)));
+        CK(cudaMalloc(&d32, h32.size() * sizeof(float)));
+        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d32, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice));
+        g_rys[device] = d;
+        g_rys32[device] = d32;
+    }
+    *rys = g_rys[device];
+    *rys32 = g_rys32[device];
+    return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Engine: the device state of builds -- task rows, counters, the
+// descriptor blob, the workspace and the per-class tuning.  A plan owns one
+// for its own builds; a batch owns one for builds over many plans.
+// ---------------------------------------------------------------------------
+struct ClassTune {
+    int tasks_per_sm;    // tasks per SM the task size aims at
+    int blocks_per_sm;   // cap on resident blocks per SM (0: occupancy limit)
+};
+
+struct Engine {
+    int device = 0, num_sms = 148;
+    int *d_rows = nullptr;          // 4 x max_rows: candidates, chunks, chunk prefix, candidate prefix
+    long long max_rows = 0;
+    void *d_cub = nullptr;
+    size_t cub_bytes = 0;
+    int *d_chunk = nullptr;         // task size per class
+    int *d_counters = nullptr;      // task counter per class
+    unsigned long long *d_nq = nullptr;   // quartets, primitive quartets, FP32 quartets per class
+    int *d_error = nullptr;         // {code, item}
+    char *h_blob = nullptr;         // pinned staging copy of the descriptors
+    char *d_blob = nullptr;
+    size_t blob_cap = 0;
+    std::vector<char> blob;         // descriptors of the build being prepared
+    std::vector<char> blob_dev;     // descriptors on the device
+    cudaEvent_t blob_ev = nullptr;  // after the last descriptor upload
+    cudaEvent_t done_ev = nullptr;  // at the end of the last build
+    bool blob_ev_rec = false, done_ev_rec = false;
+    cudaStream_t done_stream = nullptr;
+    char *d_ws = nullptr;
+    size_t ws_size = 0;
+    unsigned alloc_gen = 0;         // bumped whenever a buffer moves
+    ClassTune tune[JK_NCLASSES];
+    unsigned tune_gen = 0;
+    int shard_rank = 0, shard_size = 1;
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;    // 2 per class
+    std::vector<char> ev_used;
+    int launches = 0;
+    cudaStream_t last_stream = nullptr;
+    const double *rys = nullptr;
+    const float *rys32 = nullptr;
+    // layout of the prepared build
+    int nitems = 0;
+    int cls_view0[JK_NCLASSES], cls_nview[JK_NCLASSES], cls_rows[JK_NCLASSES],
+        cls_maxprim[JK_NCLASSES];
+    size_t off_views = 0, off_row0 = 0, off_pre = 0, off_post = 0, off_cond = 0;
+    int npre = 0, npost = 0;
+    long long pre_tiles = 0, post_tiles = 0, cond_blocks = 0;
+    char *ws = nullptr;             // workspace of the prepared build
+    size_t acc_bytes = 0;           // accumulators at its start (cleared per build)
+};
+
+struct jk_plan {
+    int device = 0;
+    int nbas_user = 0, nbas = 0, nao = 0;
+    bool expanded = false;          // a general contraction was split
+    std::vector<int> sh_l, sh_ao, sh_user;
+    double tol = 1e-13;
+    float log_tol = 0.f;
+    float q_max = -INFINITY, q_drop_max = -INFINITY;
+    long long npairs = 0;
+    long long max_rows = 0;         // largest bra-class pairs x ket-class sub-lists
+    size_t table_bytes = 0;         // device memory of the plan's tables
+    int pc_off[NPAIR_CLASSES + 1] = {0};
+    int pc_maxprim[NPAIR_CLASSES] = {0};
+    std::vector<float> q_full;      // nbas x nbas (expanded numbering)
+    // device tables
+    ShellDev *d_shells = nullptr;
+    double *d_basis = nullptr;
+    double *d_prim = nullptr;
+    PairRec *d_pairs = nullptr;
+    int *d_sh_ao = nullptr, *d_sh_nf = nullptr;
+    // ket sub-lists (equal primitive-pair count) per pair class
+    std::vector<int2> subs;
+    int sub_off[NPAIR_CLASSES + 1] = {0};
+    int2 *d_subs = nullptr;
+    double *d_io = nullptr;         // device buffers of jk_build_host
+    size_t io_size = 0;
+    Engine eng;                     // the plan's own builds
+};
+
+struct jk_batch {
+    Engine eng;
+    cudaStream_t cap_stream = nullptr;   // capture stream of the graph
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<char> graph_blob;
+    unsigned graph_alloc_gen = 0, graph_tune_gen = 0;
+    int graph_spec[4] = {0, 0, 0, 0};
+    double graph_mixed = 0;
+    int graph_launches = 0;
+    bool warmed = false;            // one build ran outside a capture
+    int last_replayed = 0, last_captured = 0;
+};
+
+// ---------------------------------------------------------------------------
+// engine allocation
+// ---------------------------------------------------------------------------
+static void engine_defaults(Engine &E)
+{
+    for (int c = 0; c < JK_NCLASSES; ++c) {
+        E.tune[c].tasks_per_sm = jk_class_table[c].form == 0 ? 64 : 16;
+        E.tune[c].blocks_per_sm = 0;
+    }
+}
+
+static int engine_init(Engine &E, int device)
+{
+    E.device = device;
+    engine_defaults(E);
+    CK(cudaDeviceGetAttribute(&E.num_sms, cudaDevAttrMultiProcessorCount, device));
+    RC(rys_tables(device, &E.rys, &E.rys32));
+    CK(cudaMalloc(&E.d_chunk, JK_NCLASSES * sizeof(int)));
+    CK(cudaMalloc(&E.d_counters, JK_NCLASSES * sizeof(int)));
+    CK(cudaMalloc(&E.d_nq, 3 * JK_NCLASSES * sizeof(unsigned long long)));
+    CK(cudaMemset(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long)));
+    CK(cudaMalloc(&E.d_error, 2 * sizeof(int)));
+    CK(cudaMemset(E.d_error, 0, 2 * sizeof(int)));
+    CK(cudaEventCreateWithFlags(&E.blob_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&E.done_ev, cudaEventDisableTiming));
+    return JK_OK;
+}
+
+static void engine_free(Engine &E)
+{
+    cudaFree(E.d_rows);
+    cudaFree(E.d_cub);
+    cudaFree(E.d_chunk);
+    cudaFree(E.d_counters);
+    cudaFree(E.d_nq);
+    cudaFree(E.d_error);
+    cudaFree(E.d_blob);
+    cudaFree(E.d_ws);
+    if (E.h_blob) cudaFreeHost(E.h_blob);
+    if (E.blob_ev) cudaEventDestroy(E.blob_ev);
+    if (E.done_ev) cudaEventDestroy(E.done_ev);
+    for (auto &e : E.ev) cudaEventDestroy(e);
+    E = Engine();
+}
+
+// wait until the device no longer uses the engine's buffers
+static int engine_idle(Engine &E)
+{
+    if (E.done_ev_rec) CK(cudaEventSynchronize(E.done_ev));
+    if (E.blob_ev_rec) CK(cudaEventSynchronize(E.blob_ev));
+    return JK_OK;
+}
+
+static int engine_reserve_rows(Engine &E, long long rows, bool no_alloc, const char *who)
+{
+    if (rows <= E.max_rows) return JK_OK;
+    if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": task rows beyond the plan's reservation");
+    RC(engine_idle(E));
+    cudaFree(E.d_rows);
+    cudaFree(E.d_cub);
+    E.d_rows = nullptr;
+    E.d_cub = nullptr;
+    E.max_rows = 0;
+    E.alloc_gen++;
+    size_t cub = 0;
+    CK(cub::DeviceScan::InclusiveSum(nullptr, cub, (int *)nullptr, (int *)nullptr, (int)rows));
+    if (cudaMalloc(&E.d_rows, 4 * (size_t)rows * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E.d_cub, std::max<size_t>(16, cub)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(JK_ERR_NOMEM, std::string(who) + ": cannot allocate the task rows");
+    }
+    E.cub_bytes = cub;
+    E.max_rows = rows;
+    return JK_OK;
+}
+
+static int engine_reserve_blob(Engine &E, size_t bytes, bool no_alloc, const char *who)
+{
+    if (bytes <= E.blob_cap) return JK_OK;
+    if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": descriptors beyond the plan's reservation");
+    RC(engine_idle(E));
+    cudaFree(E.d_blob);
+    if (E.h_blob) cudaFreeHost(E.h_blob);
+    E.d_blob = nullptr;
+    E.h_blob = nullptr;
+    E.blob_cap = 0;
+    E.blob_dev.clear();
+    E.blob_ev_rec = false;
+    E.alloc_gen++;
+    const size_t cap = align256(bytes + bytes / 4);
+    if (cudaMalloc(&E.d_blob, cap) != cudaSuccess || cudaMallocHost(&E.h_blob, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(JK_ERR_NOMEM, std::string(who) + ": cannot allocate the build descriptors");
+    }
+    E.blob_cap = cap;
+    return JK_OK;
+}
+
+// bytes of a descriptor blob
+static size_t blob_bytes(size_t nviews, size_t npre, size_t npost, size_t ncond)
+{
+    return align256(nviews * sizeof(PlanView)) + align256(nviews * sizeof(int)) +
+           align256(npre * sizeof(TileOp)) + align256(npost * sizeof(TileOp)) +
+           align256(ncond * sizeof(CondItem));
+}
+
+// ---------------------------------------------------------------------------
+// build preparation (host) and launch stream (device)
+// ---------------------------------------------------------------------------
+struct Item {
+    jk_plan *p;
+    const double *dm;
+    int n_dm;
+    double *vj, *vk;
+    // derived
+    int n_k = 0, n_j = 0, n_ka = 0;
+    bool need_t = false;
+    double *Kh = nullptr, *Jh = nullptr, *dsJ = nullptr, *DT = nullptr;
+    float *dmc = nullptr, *dm_max = nullptr;
+};
+
+struct Spec {
+    int hermi, with_j, with_k;
+    double mixed_threshold;
+};
+
+static int check_spec(const Spec &s, const char *who)
+{
+    if (s.hermi < 0 || s.hermi > 2)
+        return fail(JK_ERR_ARG, std::string(who) + ": hermi must be 0, 1 or 2");
+    return JK_OK;
+}
+
+template <class T>
+static void put(std::vector<char> &blob, size_t off, const std::vector<T> &v)
+{
+    if (!v.empty()) std::memcpy(blob.data() + off, v.data(), v.size() * sizeof(T));
+}
+
+// Lays out the workspace and the descriptors of a build over `items`.
+// ws_ext: a caller-owned workspace of ws_ext_size bytes instead of the
+// engine's; no_alloc: fail instead of growing any engine buffer.
+static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, char *ws_ext,
+                          size_t ws_ext_size, bool no_alloc, const char *who)
+{
+    RC(check_spec(s, who));
+    const int n = (int)items.size();
+    if (n <= 0) return fail(JK_ERR_ARG, std::string(who) + ": no items");
+    // ---- workspace: accumulators of every item, then per-item buffers ----
+    size_t acc = 0, need = 0;
+    for (int i = 0; i < n; ++i) {
+        Item &it = items[i];
+        if (!it.p) return fail(JK_ERR_ARG, std::string(who) + ": plan is NULL");
+        if (it.p->device != E.device)
+            return fail(JK_ERR_ARG, std::string(who) + ": plan " + std::to_string(i) +
+                                        " lives on another device");
+        if (it.n_dm <= 0 || !it.dm) return fail(JK_ERR_ARG, std::string(who) + ": no densities");
+        if ((s.with_j && !it.vj) || (s.with_k && !it.vk))
+            return fail(JK_ERR_ARG, std::string(who) + ": output is NULL");
+        const size_t nao2 = (size_t)it.p->nao * it.p->nao;
+        it.n_k = s.with_k ? (s.hermi == 0 ? 2 * it.n_dm : it.n_dm) : 0;
+        it.n_j = (s.with_j && s.hermi != 2) ? it.n_dm : 0;
+        it.n_ka = it.n_k ? it.n_dm : 0;
+        it.need_t = s.with_k && s.hermi == 0;
+        acc += align256((size_t)it.n_k * nao2 * 8) + align256((size_t)it.n_j * nao2 * 8);
+    }
+    need = acc;
+    for (const Item &it : items) {
+        const size_t nao2 = (size_t)it.p->nao * it.p->nao;
+        need += align256((size_t)it.n_j * nao2 * 8) +
+                align256(it.need_t ? (size_t)it.n_dm * nao2 * 8 : 0) +
+                align256((size_t)it.p->nbas * it.p->nbas * 4);
+    }
+    need += align256((size_t)n * 4);
+    char *ws = nullptr;
+    if (ws_ext) {
+        if (need > ws_ext_size)
+            return fail(JK_ERR_RANGE, std::string(who) + ": this build needs " + std::to_string(need) +
+                                          " bytes of scratch, the library's static scratch holds " +
+                                          std::to_string(ws_ext_size) +
+                                          " (use jk_build for larger molecules or more densities)");
+        ws = ws_ext;
+    } else {
+        if (need > E.ws_size) {
+            if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": workspace beyond reservation");
+            RC(engine_idle(E));
+            cudaFree(E.d_ws);
+            E.d_ws = nullptr;
+            E.ws_size = 0;
+            E.alloc_gen++;
+            if (cudaMalloc(&E.d_ws, need) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(JK_ERR_NOMEM, std::string(who) + ": cannot allocate " +
+                                              std::to_string(need) + " bytes of workspace");
+            }
+            E.ws_size = need;
+        }
+        ws = E.d_ws;
+    }
+    size_t o = 0;
+    for (Item &it : items) {
+        const size_t nao2 = (size_t)it.p->nao * it.p->nao;
+        it.Kh = (double *)(ws + o);
+        o += align256((size_t)it.n_k * nao2 * 8);
+        it.Jh = (double *)(ws + o);
+        o += align256((size_t)it.n_j * nao2 * 8);
+    }
+    for (Item &it : items) {
+        const size_t nao2 = (size_t)it.p->nao * it.p->nao;
+        it.dsJ = (double *)(ws + o);
+        o += align256((size_t)it.n_j * nao2 * 8);
+        it.DT = (double *)(ws + o);
+        o += align256(it.need_t ? (size_t)it.n_dm * nao2 * 8 : 0);
+        it.dmc = (float *)(ws + o);
+        o += align256((size_t)it.p->nbas * it.p->nbas * 4);
+    }
+    float *dm_max = (float *)(ws + o);
+    for (int i = 0; i < n; ++i) items[i].dm_max = dm_max + i;
+    E.ws = ws;
+    E.acc_bytes = acc;
+    E.nitems = n;
+
+    // ---- class views ----
+    const float log_mixed = s.mixed_threshold > 0 ? (float)std::log(s.mixed_threshold) : -INFINITY;
+    bool any = false;
+    for (const Item &it : items) any = any || it.n_j || it.n_k;
+    std::vector<PlanView> views;
+    std::vector<int> row0;
+    long long max_rows = 0;
+    for (int c = 0; c < JK_NCLASSES; ++c) {
+        const ClassEntry &ce = jk_class_table[c];
+        const int A = ce.bra_class, B = ce.ket_class;
+        E.cls_view0[c] = (int)views.size();
+        long long rows = 0;
+        int maxprim = 0;
+        for (const Item &it : items) {
+            if (!any) break;
+            const jk_plan *p = it.p;
+            const int nbra = p->pc_off[A + 1] - p->pc_off[A];
+            const int nket = p->pc_off[B + 1] - p->pc_off[B];
+            const int nsub = p->sub_off[B + 1] - p->sub_off[B];
+            if (nbra == 0 || nket == 0) continue;
+            PlanView v;
+            v.bra = p->d_pairs + p->pc_off[A];
+            v.ket = p->d_pairs + p->pc_off[B];
+            v.sub = p->d_subs + p->sub_off[B];
+            v.prim = p->d_prim;
+            v.dm_cond = it.dmc;
+            v.dm_max = it.dm_max;
+            v.dmK = it.dm;
+            v.dmKT = it.DT;
+            v.dsJ = it.dsJ;
+            v.Kh = it.Kh;
+            v.Jh = it.Jh;
+            v.nbra = nbra;
+            v.nket = nket;
+            v.nsub = nsub;
+            v.same_class = A == B;
+            v.nbas = p->nbas;
+            v.nao = p->nao;
+            v.n_ka = it.n_ka;
+            v.n_k = it.n_k;
+            v.n_j = it.n_j;
+            v.log_tol = p->log_tol;
+            v.mixed_log_thr = log_mixed;
+            v.row0 = (int)rows;
+            rows += (long long)nbra * nsub;
+            if (rows > INT_MAX) return fail(JK_ERR_ARG, std::string(who) + ": too many task rows");
+            maxprim = std::max(maxprim, p->pc_maxprim[A]);
+            views.push_back(v);
+            row0.push_back(v.row0);
+        }
+        E.cls_nview[c] = (int)views.size() - E.cls_view0[c];
+        E.cls_rows[c] = (int)rows;
+        E.cls_maxprim[c] = maxprim;
+        max_rows = std::max(max_rows, rows);
+    }
+    // ---- density preparation, screening and assembly descriptors ----
+    std::vector<TileOp> pre, post;
+    std::vector<CondItem> cond;
+    long long pre_tiles = 0, post_tiles = 0, cblk = 0;
+    auto op = [](const double *a, const double *b, double *out, double *outT, double f, int nao,
+                 int nd, long long &tiles) {
+        TileOp t;
+        t.a = a;
+        t.b = b;
+        t.out = out;
+        t.outT = outT;
+        t.f = f;
+        t.n = nao;
+        t.nd = nd;
+        t.nt = (nao + 31) / 32;
+        t.tile0 = tiles;
+        tiles += (long long)nd * t.nt * t.nt;
+        return t;
+    };
+    for (const Item &it : items) {
+        const int nao = it.p->nao;
+        const size_t nao2 = (size_t)nao * nao;
+        if (it.n_j || it.need_t)   // D + D^T for J, D^T for the K of hermi 0
+            pre.push_back(op(it.dm, it.dm, it.n_j ? it.dsJ : nullptr, it.need_t ? it.DT : nullptr,
+                             1.0, nao, it.n_dm, pre_tiles));
+        if (s.with_j)              // J = J_h + J_h^T (zero for hermi 2)
+            post.push_back(it.n_j ? op(it.Jh, it.Jh, it.vj, nullptr, 1.0, nao, it.n_dm, post_tiles)
+                                  : op(nullptr, nullptr, it.vj, nullptr, 0.0, nao, it.n_dm, post_tiles));
+        if (s.with_k) {            // K = K_h(D) + K_h(D^T)^T, or K_h +- K_h^T
+            if (s.hermi == 0)
+                post.push_back(op(it.Kh, it.Kh + (size_t)it.n_dm * nao2, it.vk, nullptr, 1.0, nao,
+                                  it.n_dm, post_tiles));
+            else
+                post.push_back(op(it.Kh, it.Kh, it.vk, nullptr, s.hermi == 2 ? -1.0 : 1.0, nao,
+                                  it.n_dm, post_tiles));
+        }
+        CondItem ci;
+        ci.dm = it.dm;
+        ci.sh_ao = it.p->d_sh_ao;
+        ci.sh_nf = it.p->d_sh_nf;
+        ci.dmc = it.dmc;
+        ci.dm_max = it.dm_max;
+        ci.n_dm = it.n_dm;
+        ci.nao = nao;
+        ci.nbas = it.p->nbas;
+        ci.nt = (it.p->nbas + 15) / 16;
+        ci.blk0 = cblk;
+        ci.q_drop = it.p->q_drop_max;
+        ci.q_max = it.p->q_max;
+        ci.log_tol = it.p->log_tol;
+        ci.pad = 0;
+        cblk += (long long)ci.nt * ci.nt;
+        cond.push_back(ci);
+    }
+    if (pre_tiles > INT_MAX || post_tiles > INT_MAX || cblk > INT_MAX)
+        return fail(JK_ERR_ARG, std::string(who) + ": build too large");
+    E.npre = (int)pre.size();
+    E.npost = (int)post.size();
+    E.pre_tiles = pre_tiles;
+    E.post_tiles = post_tiles;
+    E.cond_blocks = cblk;
+    E.off_views = 0;
+    E.off_row0 = E.off_views + align256(views.size() * sizeof(PlanView));
+    E.off_pre = E.off_row0 + align256(row0.size() * sizeof(int));
+    E.off_post = E.off_pre + align256(pre.size() * sizeof(TileOp));
+    E.off_cond = E.off_post + align256(post.size() * sizeof(TileOp));
+    const size_t total = E.off_cond + align256(cond.size() * sizeof(CondItem));
+    E.blob.assign(total, 0);
+    put(E.blob, E.off_views, views);
+    put(E.blob, E.off_row0, row0);
+    put(E.blob, E.off_pre, pre);
+    put(E.blob, E.off_post, post);
+    put(E.blob, E.off_cond, cond);
+    RC(engine_reserve_rows(E, std::max<long long>(1, max_rows), no_alloc, who));
+    RC(engine_reserve_blob(E, total, no_alloc, who));
+    return JK_OK;
+}
+
+// Orders this build after the engine's previous one when that ran on
+// another stream, and uploads the descriptors unless the device already
+// holds the same.  Not for a capturing stream.
+static int engine_upload(Engine &E, cudaStream_t st)
+{
+    if (E.done_ev_rec && E.done_stream != st) CK(cudaStreamWaitEvent(st, E.done_ev, 0));
+    if (E.blob == E.blob_dev) return JK_OK;
+    if (E.blob_ev_rec) CK(cudaEventSynchronize(E.blob_ev));   // staging copy free again
+    std::memcpy(E.h_blob, E.blob.data(), E.blob.size());
+    CK(cudaMemcpyAsync(E.d_blob, E.h_blob, E.blob.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(E.blob_ev, st));
+    E.blob_ev_rec = true;
+    E.blob_dev = E.blob;
+    return JK_OK;
+}
+
+static ClassArgs class_args(const Engine &E, int c)
+{
+    ClassArgs a;
+    if (E.cls_nview[c] > 0)
+        std::memcpy(&a.v0, E.blob.data() + E.off_views + E.cls_view0[c] * sizeof(PlanView),
+                    sizeof(PlanView));
+    else
+        std::memset(&a.v0, 0, sizeof(PlanView));
+    a.views = (const PlanView *)(E.d_blob + E.off_views) + E.cls_view0[c];
+    a.view_row0 = (const int *)(E.d_blob + E.off_row0) + E.cls_view0[c];
+    a.nviews = E.cls_nview[c];
+    a.nrows = E.cls_rows[c];
+    a.max_bra_prim = E.cls_maxprim[c];
+    a.shard_rank = E.shard_rank;
+    a.shard_size = E.shard_size;
+    a.rys = E.rys;
+    a.rys32 = E.rys32;
+    a.counter = E.d_counters + c;
+    a.chunk = E.d_chunk + c;
+    a.row_ncand = E.d_rows;
+    a.row_prefix = E.d_rows + 2 * E.max_rows;
+    a.nquartets = E.d_nq + c;
+    a.nprimq = E.d_nq + JK_NCLASSES + c;
+    a.nquartets32 = E.d_nq + 2 * JK_NCLASSES + c;
+    return a;
+}
+
+// Sets the launch attributes of every class kernel the prepared build uses
+// (nothing is launched): a stream capture then changes no kernel state.
+static int engine_configure(Engine &E)
+{
+    char msg[256] = {0};
+    LaunchCfg cfg;
+    cfg.stream = nullptr;
+    cfg.device = E.device;
+    cfg.num_sms = E.num_sms;
+    cfg.blocks_per_sm = 0;
+    cfg.configure_only = 1;
+    cfg.msg = msg;
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    for (int c = 0; c < JK_NCLASSES; ++c) {
+        if (!E.cls_nview[c]) continue;
+        const int rc = jk_class_table[c].launch(class_args(E, c), cfg);
+        if (rc) return fail(JK_ERR_CUDA, std::string("class kernel configuration failed: ") + msg);
+    }
+    return JK_OK;
+}
+
+// The launch stream of a prepared build (stream operations only, so that it
+// can be captured).
+static int engine_launch(Engine &E, cudaStream_t st, bool timing)
+{
+    E.launches = 0;
+    if (timing) std::fill(E.ev_used.begin(), E.ev_used.end(), 0);
+    const TileOp *d_pre = (const TileOp *)(E.d_blob + E.off_pre);
+    const TileOp *d_post = (const TileOp *)(E.d_blob + E.off_post);
+    const CondItem *d_cond = (const CondItem *)(E.d_blob + E.off_cond);
+    if (E.acc_bytes) CK(cudaMemsetAsync(E.ws, 0, E.acc_bytes, st));
+    if (E.npre) {
+        tile_op_kernel<<<(unsigned)E.pre_tiles, dim3(32, 8), 0, st>>>(d_pre, E.npre);
+        CK(cudaGetLastError());
+        E.launches++;
+    }
+    dm_cond_kernel<<<(unsigned)E.cond_blocks, dim3(16, 16), 0, st>>>(d_cond, E.nitems);
+    CK(cudaGetLastError());
+    dm_max_kernel<<<E.nitems, 256, 0, st>>>(d_cond, E.d_error);
+    CK(cudaGetLastError());
+    E.launches += 2;
+    CK(cudaMemsetAsync(E.d_counters, 0, JK_NCLASSES * sizeof(int), st));
+    CK(cudaMemsetAsync(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
+    char msg[256] = {0};
+    LaunchCfg cfg;
+    cfg.stream = st;
+    cfg.device = E.device;
+    cfg.num_sms = E.num_sms;
+    cfg.configure_only = 0;
+    cfg.msg = msg;
+    int *chunks = E.d_rows + E.max_rows;
+    int *prefix = E.d_rows + 2 * E.max_rows;
+    int *cand_prefix = E.d_rows + 3 * E.max_rows;
+    for (int c = 0; c < JK_NCLASSES; ++c) {
+        const int rows = E.cls_rows[c];
+        if (!E.cls_nview[c] || rows == 0) continue;
+        const ClassEntry &ce = jk_class_table[c];
+        const ClassArgs a = class_args(E, c);
+        if (timing) CK(cudaEventRecord(E.ev[2 * c], st));
+        // task list: candidates per row, a task size giving about
+        // tasks_per_sm tasks per SM, chunks per row, prefix sum of chunks
+        task_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(a, E.d_rows);
+        CK(cudaGetLastError());
+        size_t tmp = E.cub_bytes;
+        CK(cub::DeviceScan::InclusiveSum(E.d_cub, tmp, E.d_rows, cand_prefix, rows, st));
+        const int lo = ce.form == 0 ? 128 : 32, hi = ce.form == 0 ? 4096 : 1024;
+        const int target = std::max(1, E.tune[c].tasks_per_sm) * E.num_sms;
+        task_chunks_kernel<<<(rows + 255) / 256, 256, 0, st>>>(E.d_rows, cand_prefix, rows, target,
+                                                               lo, hi, E.d_chunk + c, chunks);
+        CK(cudaGetLastError());
+        tmp = E.cub_bytes;
+        CK(cub::DeviceScan::InclusiveSum(E.d_cub, tmp, chunks, prefix, rows, st));
+        E.launches += 4;
+        cfg.blocks_per_sm = E.tune[c].blocks_per_sm;
+        int rc;
+        {
+            std::lock_guard<std::mutex> lock(g_launch_mutex);
+            rc = ce.launch(a, cfg);
+        }
+        if (rc != 0)
+            return fail(JK_ERR_CUDA, std::string("class kernel launch failed: ") + msg + " " +
+                                         cudaGetErrorString((cudaError_t)rc));
+        E.launches++;
+        if (timing) {
+            CK(cudaEventRecord(E.ev[2 * c + 1], st));
+            E.ev_used[c] = 1;
+        }
+    }
+    if (E.npost) {
+        tile_op_kernel<<<(unsigned)E.post_tiles, dim3(32, 8), 0, st>>>(d_post, E.npost);
+        CK(cudaGetLastError());
+        E.launches++;
+    }
+    return JK_OK;
+}
+
+static int engine_finish(Engine &E, cudaStream_t st)
+{
+    CK(cudaEventRecord(E.done_ev, st));
+    E.done_ev_rec = true;
+    E.done_stream = st;
+    E.last_stream = st;
+    return JK_OK;
+}
+
+// prepare, upload and launch a build outside any capture
+static int engine_build(Engine &E, std::vector<Item> &items, const Spec &s, cudaStream_t st,
+                        char *ws_ext, size_t ws_ext_size, bool no_alloc, const char *who)
+{
+    RC(engine_prepare(E, items, s, ws_ext, ws_ext_size, no_alloc, who));
+    RC(engine_upload(E, st));
+    RC(engine_launch(E, st, E.timing));
+    return engine_finish(E, st);
+}
+
+static int engine_sync(Engine &E, cudaStream_t st, const char *who)
+{
+    CK(cudaStreamSynchronize(st));
+    int err[2] = {0, 0};
+    CK(cudaMemcpy(err, E.d_error, sizeof(err), cudaMemcpyDeviceToHost));
+    if (err[0]) {
+        CK(cudaMemset(E.d_error, 0, sizeof(err)));
+        if (err[0] == JK_ERR_RANGE)
+            return fail(JK_ERR_RANGE, std::string(who) + ": density elements of item " +
+                                          std::to_string(err[1]) +
+                                          " exceed the range the plan was built for "
+                                          "(shell pairs it dropped would pass the screening)");
+        return fail(JK_ERR_DEVICE, std::string(who) + ": kernel error flag " + std::to_string(err[0]));
+    }
+    return JK_OK;
+}
+
+static int engine_counts(Engine &E, unsigned long long *quartets, unsigned long long *prim_quartets,
+                         unsigned long long *quartets_f32, int ncounts, int *nclasses)
+{
+    if (nclasses) *nclasses = JK_NCLASSES;
+    if (!quartets && !prim_quartets && !quartets_f32) return JK_OK;
+    CK(cudaStreamSynchronize(E.last_stream));
+    std::vector<unsigned long long> h(3 * JK_NCLASSES);
+    CK(cudaMemcpy(h.data(), E.d_nq, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < ncounts && k < JK_NCLASSES; ++k) {
+        if (quartets) quartets[k] = h[k];
+        if (prim_quartets) prim_quartets[k] = h[JK_NCLASSES + k];
+        if (quartets_f32) quartets_f32[k] = h[2 * JK_NCLASSES + k];
+    }
+    return JK_OK;
+}
+
+static int engine_set_timing(Engine &E, int enable)
+{
+    if (enable && E.ev.empty()) {
+        E.ev.resize(2 * JK_NCLASSES);
+        for (auto &e : E.ev) CK(cudaEventCreate(&e));
+        E.ev_used.assign(JK_NCLASSES, 0);
+    }
+    E.timing = enable != 0;
+    return JK_OK;
+}
+
+static int engine_class_ms(Engine &E, float *ms, int ncounts, int *launches)
+{
+    if (launches) *launches = E.launches;
+    if (!ms) return JK_OK;
+    CK(cudaStreamSynchronize(E.last_stream));
+    for (int c = 0; c < ncounts && c < JK_NCLASSES; ++c) {
+        ms[c] = 0.f;
+        if (E.timing && c < (int)E.ev_used.size() && E.ev_used[c])
+            CK(cudaEventElapsedTime(&ms[c], E.ev[2 * c], E.ev[2 * c + 1]));
+    }
+    return JK_OK;
+}
+
+static int engine_set_tuning(Engine &E, int cls, int tasks_per_sm, int blocks_per_sm)
+{
+    if (cls < -1 || cls >= JK_NCLASSES) return fail(JK_ERR_ARG, "tuning: no such class");
+    if (tasks_per_sm < 0 || blocks_per_sm < 0) return fail(JK_ERR_ARG, "tuning: negative value");
+    if (cls == -1) {
+        engine_defaults(E);
+    } else {
+        const int def = jk_class_table[cls].form == 0 ? 64 : 16;
+        E.tune[cls].tasks_per_sm = tasks_per_sm ? tasks_per_sm : def;
+        E.tune[cls].blocks_per_sm = blocks_per_sm;
+    }
+    E.tune_gen++;
+    return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plans
+// ---------------------------------------------------------------------------
 static void free_plan(jk_plan *p)
 {
     cudaFree(p->d_shells);
     cudaFree(p->d_basis);
     cudaFree(p->d_prim);
     cudaFree(p->d_pairs);
-    cudaFree(p->d_rys);
-    cudaFree(p->d_rys32);
     cudaFree(p->d_sh_ao);
     cudaFree(p->d_sh_nf);
-    cudaFree(p->d_counters);
-    cudaFree(p->d_nq);
-    cudaFree(p->d_error);
-    cudaFree(p->d_dm_max);
-    cudaFree(p->d_ws);
     cudaFree(p->d_io);
     cudaFree(p->d_subs);
-    cudaFree(p->d_rows);
-    cudaFree(p->d_chunk);
-    cudaFree(p->d_cub);
+    engine_free(p->eng);
 }
 
 template <class T>
-static cudaError_t upload(T **dst, const std::vector<T> &src)
+static cudaError_t upload(T **dst, const std::vector<T> &src, cudaStream_t st, size_t *bytes_out)
 {
-    size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
+    const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
     cudaError_t e = cudaMalloc((void **)dst, bytes);
     if (e != cudaSuccess) return e;
-    if (!src.empty()) e = cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (bytes_out) *bytes_out += bytes;
+    if (!src.empty())
+        e = cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
     return e;
 }
+
+// owns the private stream and the temporaries of a plan construction
+struct PlanScratch {
+    cudaStream_t st = nullptr;
+    int4 *d_rec = nullptr, *d_cand = nullptr;
+    float *d_q = nullptr;
+    ~PlanScratch()
+    {
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaFreeAsync(d_rec, st);
+            cudaFreeAsync(d_cand, st);
+            cudaFreeAsync(d_q, st);
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    }
+};
 
 static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, const double *env,
                        const int *ao_loc, double tol, int device, jk_plan *p)
@@ -150,7 +856,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     p->tol = tol;
     p->log_tol = (float)std::log(tol);
     p->nbas_user = nbas_user;
-    CK(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device));
+    RC(engine_init(p->eng, device));
 
     // ---- shells (general contractions expanded, contraction-major) ----
     std::vector<ShellDev> shells;
@@ -212,44 +918,38 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     }
     if ((long long)rec.size() > (1ll << 31) - 1) return fail(JK_ERR_ARG, "molecule too large");
 
-    CK(upload(&p->d_shells, shells));
-    CK(upload(&p->d_basis, basis));
-    int4 *d_rec = nullptr, *d_cand = nullptr;
-    float *d_q = nullptr;
-    CK(upload(&d_rec, rec));
-    CK(upload(&d_cand, cand));
-    CK(cudaMalloc(&p->d_prim, std::max<size_t>(1, rec.size()) * JK_PRIM_STRIDE * sizeof(double)));
-    CK(cudaMalloc(&d_q, std::max<size_t>(1, cand.size()) * sizeof(float)));
-
-    std::vector<double> rys_host(RYS_TOTAL);
-    std::memcpy(rys_host.data(), rys_table_host, sizeof(rys_table_host));
-    std::vector<float> rys32_host(RYS32_TOTAL);
-    std::memcpy(rys32_host.data(), rys_table32_host, sizeof(rys_table32_host));
-    for (int n = 0; n < RYS_NMAX; ++n)
-        for (int k = 0; k < RYS_NMAX; ++k) {
-            rys_host[RYS_LARGEX_OFF + n * RYS_NMAX + k] = rys_largex_r_host[n][k];
-            rys_host[RYS_LARGEX_OFF + RYS_NMAX * RYS_NMAX + n * RYS_NMAX + k] = rys_largex_w_host[n][k];
-            rys32_host[RYS32_LARGEX_OFF + n * RYS_NMAX + k] = (float)rys_largex_r_host[n][k];
-            rys32_host[RYS32_LARGEX_OFF + RYS_NMAX * RYS_NMAX + n * RYS_NMAX + k] =
-                (float)rys_largex_w_host[n][k];
-        }
-    CK(upload(&p->d_rys, rys_host));
-    CK(upload(&p->d_rys32, rys32_host));
+    // the construction runs on a private stream, so that it does not wait
+    // for (or hold up) builds of other plans on the caller's streams
+    PlanScratch tmp;
+    CK(cudaStreamCreateWithFlags(&tmp.st, cudaStreamNonBlocking));
+    const cudaStream_t st = tmp.st;
+    CK(upload(&p->d_shells, shells, st, &p->table_bytes));
+    CK(upload(&p->d_basis, basis, st, &p->table_bytes));
+    CK(cudaMallocAsync(&tmp.d_rec, std::max<size_t>(1, rec.size()) * sizeof(int4), st));
+    CK(cudaMallocAsync(&tmp.d_cand, std::max<size_t>(1, cand.size()) * sizeof(int4), st));
+    CK(cudaMallocAsync(&tmp.d_q, std::max<size_t>(1, cand.size()) * sizeof(float), st));
+    if (!rec.empty())
+        CK(cudaMemcpyAsync(tmp.d_rec, rec.data(), rec.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    if (!cand.empty())
+        CK(cudaMemcpyAsync(tmp.d_cand, cand.data(), cand.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                           st));
+    const size_t prim_bytes = std::max<size_t>(1, rec.size()) * JK_PRIM_STRIDE * sizeof(double);
+    CK(cudaMalloc(&p->d_prim, prim_bytes));
+    p->table_bytes += prim_bytes;
 
     if (!rec.empty()) {
         const int nt = 256;
-        prim_pair_fill_kernel<<<(unsigned)((rec.size() + nt - 1) / nt), nt>>>(
-            d_rec, (long long)rec.size(), p->d_shells, p->d_basis, p->d_prim);
+        prim_pair_fill_kernel<<<(unsigned)((rec.size() + nt - 1) / nt), nt, 0, st>>>(
+            tmp.d_rec, (long long)rec.size(), p->d_shells, p->d_basis, p->d_prim);
         CK(cudaGetLastError());
-        schwarz_kernel<<<(unsigned)((cand.size() + 127) / 128), 128>>>(
-            d_cand, (int)cand.size(), p->d_shells, p->d_prim, p->d_rys, d_q);
+        schwarz_kernel<<<(unsigned)((cand.size() + 127) / 128), 128, 0, st>>>(
+            tmp.d_cand, (int)cand.size(), p->d_shells, p->d_prim, p->eng.rys, tmp.d_q);
         CK(cudaGetLastError());
     }
     std::vector<float> q(cand.size());
-    if (!cand.empty()) CK(cudaMemcpy(q.data(), d_q, q.size() * sizeof(float), cudaMemcpyDeviceToHost));
-    cudaFree(d_rec);
-    cudaFree(d_cand);
-    cudaFree(d_q);
+    if (!cand.empty())
+        CK(cudaMemcpyAsync(q.data(), tmp.d_q, q.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
 
     // ---- keep, classify, sort ----
     float qmax = -INFINITY;
@@ -305,8 +1005,8 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     }
     p->pc_off[NPAIR_CLASSES] = (int)recs.size();
     p->sub_off[NPAIR_CLASSES] = (int)p->subs.size();
-    CK(upload(&p->d_subs, p->subs));
-    // task rows: the largest (bra class pairs) x (ket class sub-lists)
+    CK(upload(&p->d_subs, p->subs, st, &p->table_bytes));
+    // task rows of one class: the largest (bra class pairs) x (ket class sub-lists)
     long long max_rows = 1;
     for (int A = 0; A < NPAIR_CLASSES; ++A)
         for (int B = 0; B <= A; ++B)
@@ -314,26 +1014,18 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
                 max_rows, (long long)(p->pc_off[A + 1] - p->pc_off[A]) *
                               (p->sub_off[B + 1] - p->sub_off[B]));
     if (max_rows > (1ll << 31) - 1) return fail(JK_ERR_ARG, "molecule too large (task rows)");
-    CK(cudaMalloc(&p->d_rows, 4 * (size_t)max_rows * sizeof(int)));
-    CK(cudaMalloc(&p->d_chunk, JK_NCLASSES * sizeof(int)));
     p->max_rows = max_rows;
-    p->cub_bytes = 0;
-    CK(cub::DeviceScan::InclusiveSum(nullptr, p->cub_bytes, p->d_rows, p->d_rows, (int)max_rows));
-    CK(cudaMalloc(&p->d_cub, std::max<size_t>(16, p->cub_bytes)));
     p->npairs = (long long)recs.size();
-    CK(upload(&p->d_pairs, recs));
-
+    CK(upload(&p->d_pairs, recs, st, &p->table_bytes));
     std::vector<int> nf(nbas);
     for (int s = 0; s < nbas; ++s) nf[s] = ncart(shells[s].l);
-    CK(upload(&p->d_sh_ao, p->sh_ao));
-    CK(upload(&p->d_sh_nf, nf));
-    CK(cudaMalloc(&p->d_counters, JK_NCLASSES * sizeof(int)));
-    CK(cudaMalloc(&p->d_nq, 3 * JK_NCLASSES * sizeof(unsigned long long)));
-    CK(cudaMalloc(&p->d_error, sizeof(int)));
-    CK(cudaMemset(p->d_error, 0, sizeof(int)));
-    CK(cudaMemset(p->d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long)));
-    CK(cudaMalloc(&p->d_dm_max, sizeof(float)));
-    CK(cudaDeviceSynchronize());
+    CK(upload(&p->d_sh_ao, p->sh_ao, st, &p->table_bytes));
+    CK(upload(&p->d_sh_nf, nf, st, &p->table_bytes));
+    // the plan's own builds (one item) never grow these: jk_build_noalloc
+    // relies on it
+    RC(engine_reserve_rows(p->eng, max_rows, false, "jk_plan_create"));
+    RC(engine_reserve_blob(p->eng, blob_bytes(JK_NCLASSES, 1, 2, 1), false, "jk_plan_create"));
+    CK(cudaStreamSynchronize(st));
     return JK_OK;
 }
 
@@ -343,7 +1035,8 @@ extern "C" int jk_plan_create(const int *atm, int natm, const int *bas, int nbas
     if (!out) return fail(JK_ERR_ARG, "jk_plan_create: out is NULL");
     *out = nullptr;
     int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev ||
+        device >= JK_MAX_DEVICES)
         return fail(JK_ERR_CUDA, "jk_plan_create: no CUDA device " + std::to_string(device));
     DeviceGuard g(device);
     jk_plan *p = new jk_plan();
@@ -361,7 +1054,7 @@ extern "C" int jk_plan_destroy(jk_plan *plan)
 {
     if (!plan) return JK_OK;
     DeviceGuard g(plan->device);
-    cudaDeviceSynchronize();
+    engine_idle(plan->eng);
     free_plan(plan);
     delete plan;
     return JK_OK;
@@ -375,6 +1068,16 @@ extern "C" int jk_plan_info(const jk_plan *plan, int *nao, long long *npairs)
     return JK_OK;
 }
 
+extern "C" int jk_plan_memory(const jk_plan *plan, long long *table_bytes, long long *workspace_bytes)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_plan_memory: plan is NULL");
+    if (table_bytes)
+        *table_bytes = (long long)(plan->table_bytes + 4 * (size_t)plan->eng.max_rows * sizeof(int) +
+                                   plan->eng.cub_bytes + plan->eng.blob_cap);
+    if (workspace_bytes) *workspace_bytes = (long long)(plan->eng.ws_size + plan->io_size);
+    return JK_OK;
+}
+
 extern "C" int jk_plan_q_cond(const jk_plan *plan, float *q_host, int nbas)
 {
     if (!plan || !q_host) return fail(JK_ERR_ARG, "jk_plan_q_cond: null argument");
@@ -384,186 +1087,37 @@ extern "C" int jk_plan_q_cond(const jk_plan *plan, float *q_host, int nbas)
     return JK_OK;
 }
 
-static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
-
-// ws_ext: when not NULL, the build's workspace is taken from this caller-owned
-// device buffer of ws_ext_size bytes instead of the plan's own allocation.
-static int build_impl(jk_plan *p, const double *dm, int n_dm, int hermi, int with_j, int with_k,
-                      double *vj, double *vk, double mixed_threshold, cudaStream_t st,
-                      char *ws_ext = nullptr, size_t ws_ext_size = 0)
+extern "C" int jk_plan_set_shard(jk_plan *plan, int rank, int size)
 {
-    if (n_dm <= 0 || !dm) return fail(JK_ERR_ARG, "jk_build: no densities");
-    if (hermi < 0 || hermi > 2) return fail(JK_ERR_ARG, "jk_build: hermi must be 0, 1 or 2");
-    if ((with_j && !vj) || (with_k && !vk)) return fail(JK_ERR_ARG, "jk_build: output is NULL");
-    const float log_mixed = mixed_threshold > 0 ? (float)std::log(mixed_threshold) : -INFINITY;
-    const int nao = p->nao;
-    const size_t nao2 = (size_t)nao * nao;
-    const int n_k = with_k ? (hermi == 0 ? 2 * n_dm : n_dm) : 0;
-    const int n_j = (with_j && hermi != 2) ? n_dm : 0;
-    const bool need_t = with_k && hermi == 0;
-    // workspace: Kh | Jh | dsJ | DT | dm_cond
-    const size_t o_kh = 0;
-    const size_t o_jh = o_kh + align256((size_t)n_k * nao2 * 8);
-    const size_t o_ds = o_jh + align256((size_t)n_j * nao2 * 8);
-    const size_t o_dt = o_ds + align256((size_t)n_j * nao2 * 8);
-    const size_t o_dc = o_dt + align256(need_t ? (size_t)n_dm * nao2 * 8 : 0);
-    const size_t need = o_dc + align256((size_t)p->nbas * p->nbas * 4);
-    char *ws = p->d_ws;
-    if (ws_ext) {
-        if (need > ws_ext_size)
-            return fail(JK_ERR_RANGE, "jk_build_noalloc: this build needs " + std::to_string(need) +
-                                          " bytes of scratch, the library's static scratch holds " +
-                                          std::to_string(ws_ext_size) +
-                                          " (use jk_build for larger molecules or more densities)");
-        ws = ws_ext;
-    } else if (need > p->ws_size) {
-        CK(cudaStreamSynchronize(st));
-        cudaFree(p->d_ws);
-        p->d_ws = nullptr;
-        p->ws_size = 0;
-        if (cudaMalloc(&p->d_ws, need) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(JK_ERR_NOMEM, "jk_build: cannot allocate " + std::to_string(need) +
-                                          " bytes of workspace");
-        }
-        p->ws_size = need;
-        ws = p->d_ws;
-    }
-    double *Kh = (double *)(ws + o_kh);
-    double *Jh = (double *)(ws + o_jh);
-    double *dsJ = (double *)(ws + o_ds);
-    double *DT = (double *)(ws + o_dt);
-    float *dmc = (float *)(ws + o_dc);
-    p->last_stream = st;
-    p->launches = 0;
-    if (p->timing) std::fill(p->ev_used.begin(), p->ev_used.end(), 0);
-
-    const dim3 tb(32, 8);
-    const dim3 tg((nao + 31) / 32, (nao + 31) / 32, n_dm);
-    if (n_j) {
-        add_transpose_kernel<<<tg, tb, 0, st>>>(dm, dm, 1.0, nao, dsJ);
-        CK(cudaGetLastError());
-        p->launches++;
-        CK(cudaMemsetAsync(Jh, 0, (size_t)n_j * nao2 * 8, st));
-    }
-    if (need_t) {
-        transpose_kernel<<<tg, tb, 0, st>>>(dm, nao, DT);
-        CK(cudaGetLastError());
-        p->launches++;
-    }
-    if (n_k) CK(cudaMemsetAsync(Kh, 0, (size_t)n_k * nao2 * 8, st));
-    {
-        const dim3 b2(16, 16);
-        const dim3 g2((p->nbas + 15) / 16, (p->nbas + 15) / 16);
-        dm_cond_kernel<<<g2, b2, 0, st>>>(dm, n_dm, nao, p->d_sh_ao, p->d_sh_nf, p->nbas, dmc);
-        CK(cudaGetLastError());
-        max_reduce_kernel<<<1, 1024, 0, st>>>(dmc, (long long)p->nbas * p->nbas, p->d_dm_max);
-        CK(cudaGetLastError());
-        range_check_kernel<<<1, 1, 0, st>>>(p->d_dm_max, p->q_drop_max, p->q_max, p->log_tol,
-                                           p->d_error);
-        CK(cudaGetLastError());
-        p->launches += 3;
-    }
-    CK(cudaMemsetAsync(p->d_counters, 0, JK_NCLASSES * sizeof(int), st));
-    CK(cudaMemsetAsync(p->d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
-
-    if (n_j || n_k) {
-        LaunchCfg cfg;
-        cfg.stream = st;
-        cfg.num_sms = p->num_sms;
-        cfg.blocks_per_sm = 0;
-        cfg.mixed = 0;
-        char launch_msg[256] = {0};
-        cfg.msg = launch_msg;
-        for (int c = 0; c < JK_NCLASSES; ++c) {
-            const ClassEntry &ce = jk_class_table[c];
-            const int A = ce.bra_class, B = ce.ket_class;
-            const int nbra = p->pc_off[A + 1] - p->pc_off[A];
-            const int nket = p->pc_off[B + 1] - p->pc_off[B];
-            if (nbra == 0 || nket == 0) continue;
-            ClassArgs a;
-            a.bra = p->d_pairs + p->pc_off[A];
-            a.ket = p->d_pairs + p->pc_off[B];
-            a.nbra = nbra;
-            a.nket = nket;
-            a.same_class = A == B;
-            a.max_bra_prim = p->pc_maxprim[A];
-            a.prim = p->d_prim;
-            a.rys = p->d_rys;
-            a.rys32 = p->d_rys32;
-            a.dm_cond = dmc;
-            a.nbas = p->nbas;
-            a.log_tol = p->log_tol;
-            a.dm_max = p->d_dm_max;
-            a.nao = nao;
-            a.dmK = dm;
-            a.dmKT = DT;
-            a.n_ka = n_k ? n_dm : 0;
-            a.n_k = n_k;
-            a.dsJ = dsJ;
-            a.n_j = n_j;
-            a.Kh = Kh;
-            a.Jh = Jh;
-            a.counter = p->d_counters + c;
-            a.sub = p->d_subs + p->sub_off[B];
-            a.nsub = p->sub_off[B + 1] - p->sub_off[B];
-            a.chunk = p->d_chunk + c;
-            a.row_ncand = p->d_rows;
-            int *chunks = p->d_rows + p->max_rows;
-            int *prefix = p->d_rows + 2 * p->max_rows;
-            int *cand_prefix = p->d_rows + 3 * p->max_rows;
-            a.row_prefix = prefix;
-            const int rows = nbra * a.nsub;
-            a.nquartets = p->d_nq + c;
-            a.nprimq = p->d_nq + JK_NCLASSES + c;
-            a.mixed_log_thr = log_mixed;
-            a.nquartets32 = p->d_nq + 2 * JK_NCLASSES + c;
-            a.error = p->d_error;
-            if (p->timing) CK(cudaEventRecord(p->ev[2 * c], st));
-            // task list: candidates per row, a chunk size giving ~16 tasks per
-            // SM, chunks per row, prefix sum of chunks
-            task_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(a);
-            CK(cudaGetLastError());
-            size_t tmp_bytes = p->cub_bytes;
-            CK(cub::DeviceScan::InclusiveSum(p->d_cub, tmp_bytes, p->d_rows, cand_prefix, rows, st));
-            const int lo = ce.form == 0 ? 128 : 32, hi = ce.form == 0 ? 4096 : 1024;
-            const int target = (ce.form == 0 ? 64 : 16) * p->num_sms;
-            task_chunks_kernel<<<(rows + 255) / 256, 256, 0, st>>>(
-                p->d_rows, cand_prefix, rows, target, lo, hi, p->d_chunk + c, chunks);
-            CK(cudaGetLastError());
-            tmp_bytes = p->cub_bytes;
-            CK(cub::DeviceScan::InclusiveSum(p->d_cub, tmp_bytes, chunks, prefix, rows, st));
-            p->launches += 4;
-            int rc = ce.launch(a, cfg);
-            if (rc != 0)
-                return fail(JK_ERR_CUDA, std::string("class kernel launch failed: ") + launch_msg + " " +
-                                             cudaGetErrorString((cudaError_t)rc));
-            if (p->timing) {
-                CK(cudaEventRecord(p->ev[2 * c + 1], st));
-                p->ev_used[c] = 1;
-            }
-            p->launches++;
-        }
-    }
-    // assemble J and K
-    if (with_j) {
-        if (n_j) {
-            add_transpose_kernel<<<tg, tb, 0, st>>>(Jh, Jh, 1.0, nao, vj);
-            CK(cudaGetLastError());
-            p->launches++;
-        } else {
-            CK(cudaMemsetAsync(vj, 0, (size_t)n_dm * nao2 * 8, st));
-        }
-    }
-    if (with_k) {
-        if (hermi == 0)
-            add_transpose_kernel<<<tg, tb, 0, st>>>(Kh, Kh + (size_t)n_dm * nao2, 1.0, nao, vk);
-        else
-            add_transpose_kernel<<<tg, tb, 0, st>>>(Kh, Kh, hermi == 2 ? -1.0 : 1.0, nao, vk);
-        CK(cudaGetLastError());
-        p->launches++;
-    }
+    if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_shard: plan is NULL");
+    if (size < 1 || rank < 0 || rank >= size)
+        return fail(JK_ERR_ARG, "jk_plan_set_shard: need 0 <= rank < size");
+    plan->eng.shard_rank = rank;
+    plan->eng.shard_size = size;
     return JK_OK;
+}
+
+extern "C" int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_sm)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_tuning: plan is NULL");
+    return engine_set_tuning(plan->eng, cls, tasks_per_sm, blocks_per_sm);
+}
+
+// ---------------------------------------------------------------------------
+// single-plan builds
+// ---------------------------------------------------------------------------
+static int build_one(jk_plan *p, const double *dm, int n_dm, int hermi, int with_j, int with_k,
+                     double *vj, double *vk, double mixed_threshold, cudaStream_t st, char *ws_ext,
+                     size_t ws_ext_size, bool no_alloc, const char *who)
+{
+    std::vector<Item> items(1);
+    items[0].p = p;
+    items[0].dm = dm;
+    items[0].n_dm = n_dm;
+    items[0].vj = vj;
+    items[0].vk = vk;
+    const Spec s{hermi, with_j, with_k, mixed_threshold};
+    return engine_build(p->eng, items, s, st, ws_ext, ws_ext_size, no_alloc, who);
 }
 
 extern "C" int jk_build(jk_plan *plan, const double *dm, int n_dm, int hermi, int with_j,
@@ -571,25 +1125,15 @@ extern "C" int jk_build(jk_plan *plan, const double *dm, int n_dm, int hermi, in
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_build: plan is NULL");
     DeviceGuard g(plan->device);
-    return build_impl(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
-                      (cudaStream_t)stream);
+    return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
+                     (cudaStream_t)stream, nullptr, 0, false, "jk_build");
 }
 
 extern "C" int jk_sync(jk_plan *plan, void *stream)
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_sync: plan is NULL");
     DeviceGuard g(plan->device);
-    CK(cudaStreamSynchronize((cudaStream_t)stream));
-    int err = 0;
-    CK(cudaMemcpy(&err, plan->d_error, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) {
-        CK(cudaMemset(plan->d_error, 0, sizeof(int)));
-        if (err == JK_ERR_RANGE)
-            return fail(JK_ERR_RANGE, "density elements exceed the range the plan was built for "
-                                      "(shell pairs it dropped would pass the screening)");
-        return fail(JK_ERR_DEVICE, "kernel error flag " + std::to_string(err));
-    }
-    return JK_OK;
+    return engine_sync(plan->eng, (cudaStream_t)stream, "jk_sync");
 }
 
 // ---------------------------------------------------------------------------
@@ -631,8 +1175,9 @@ extern "C" int jk_build_noalloc(jk_plan *plan, const double *dm, int n_dm, int h
     char *scratch = nullptr;
     const int rc = noalloc_scratch(plan->device, &scratch);
     if (rc) return rc;
-    return build_impl(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
-                      (cudaStream_t)stream, scratch, (size_t)JK_NOALLOC_SCRATCH_BYTES);
+    return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
+                     (cudaStream_t)stream, scratch, (size_t)JK_NOALLOC_SCRATCH_BYTES, true,
+                     "jk_build_noalloc");
 }
 
 extern "C" int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi, int with_j,
@@ -640,12 +1185,13 @@ extern "C" int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int
                              void *stream)
 {
     if (!plan || !dm_host) return fail(JK_ERR_ARG, "jk_build_host: null argument");
+    if (n_dm <= 0) return fail(JK_ERR_ARG, "jk_build_host: no densities");
     DeviceGuard g(plan->device);
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)n_dm * plan->nao * plan->nao;
     const size_t need = 3 * n * sizeof(double);
     if (need > plan->io_size) {
-        CK(cudaStreamSynchronize(st));
+        RC(engine_idle(plan->eng));
         cudaFree(plan->d_io);
         plan->d_io = nullptr;
         plan->io_size = 0;
@@ -657,9 +1203,8 @@ extern "C" int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int
     }
     double *d_dm = plan->d_io, *d_vj = d_dm + n, *d_vk = d_vj + n;
     CK(cudaMemcpyAsync(d_dm, dm_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
-    int rc = build_impl(plan, d_dm, n_dm, hermi, with_j, with_k, with_j ? d_vj : nullptr,
-                        with_k ? d_vk : nullptr, mixed_threshold, st);
-    if (rc) return rc;
+    RC(build_one(plan, d_dm, n_dm, hermi, with_j, with_k, with_j ? d_vj : nullptr,
+                 with_k ? d_vk : nullptr, mixed_threshold, st, nullptr, 0, false, "jk_build_host"));
     if (with_j && vj_host)
         CK(cudaMemcpyAsync(vj_host, d_vj, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (with_k && vk_host)
@@ -672,21 +1217,180 @@ extern "C" int jk_last_counts(jk_plan *plan, unsigned long long *quartets,
                               unsigned long long *quartets_f32, int ncounts, int *nclasses)
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_last_counts: plan is NULL");
-    if (nclasses) *nclasses = JK_NCLASSES;
-    if (!quartets && !prim_quartets && !quartets_f32) return JK_OK;
     DeviceGuard g(plan->device);
-    CK(cudaStreamSynchronize(plan->last_stream));
-    std::vector<unsigned long long> h(3 * JK_NCLASSES);
-    CK(cudaMemcpy(h.data(), plan->d_nq, 3 * JK_NCLASSES * sizeof(unsigned long long),
-                  cudaMemcpyDeviceToHost));
-    for (int k = 0; k < ncounts && k < JK_NCLASSES; ++k) {
-        if (quartets) quartets[k] = h[k];
-        if (prim_quartets) prim_quartets[k] = h[JK_NCLASSES + k];
-        if (quartets_f32) quartets_f32[k] = h[2 * JK_NCLASSES + k];
+    return engine_counts(plan->eng, quartets, prim_quartets, quartets_f32, ncounts, nclasses);
+}
+
+extern "C" int jk_set_timing(jk_plan *plan, int enable)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_set_timing: plan is NULL");
+    DeviceGuard g(plan->device);
+    return engine_set_timing(plan->eng, enable);
+}
+
+extern "C" int jk_last_class_ms(jk_plan *plan, float *ms, int ncounts, int *launches)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_last_class_ms: plan is NULL");
+    DeviceGuard g(plan->device);
+    return engine_class_ms(plan->eng, ms, ncounts, launches);
+}
+
+// ---------------------------------------------------------------------------
+// batched builds over many plans
+// ---------------------------------------------------------------------------
+extern "C" int jk_batch_create(int device, jk_batch **out)
+{
+    if (!out) return fail(JK_ERR_ARG, "jk_batch_create: out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev ||
+        device >= JK_MAX_DEVICES)
+        return fail(JK_ERR_CUDA, "jk_batch_create: no CUDA device " + std::to_string(device));
+    DeviceGuard g(device);
+    jk_batch *b = new jk_batch();
+    int rc = engine_init(b->eng, device);
+    if (rc == JK_OK && cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+        rc = fail(JK_ERR_CUDA, "jk_batch_create: cannot create the capture stream");
+    if (rc != JK_OK) {
+        engine_free(b->eng);
+        delete b;
+        return rc;
     }
+    *out = b;
     return JK_OK;
 }
 
+extern "C" int jk_batch_destroy(jk_batch *batch)
+{
+    if (!batch) return JK_OK;
+    DeviceGuard g(batch->eng.device);
+    engine_idle(batch->eng);
+    if (batch->gexec) cudaGraphExecDestroy(batch->gexec);
+    if (batch->cap_stream) cudaStreamDestroy(batch->cap_stream);
+    engine_free(batch->eng);
+    delete batch;
+    return JK_OK;
+}
+
+extern "C" int jk_batch_build(jk_batch *batch, jk_plan *const *plans, int nplans,
+                              const double *const *dms, const int *n_dm, int hermi, int with_j,
+                              int with_k, double *const *vj, double *const *vk,
+                              double mixed_threshold, int use_graph, void *stream)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_build: batch is NULL");
+    if (!plans || !dms || !n_dm || nplans <= 0)
+        return fail(JK_ERR_ARG, "jk_batch_build: empty batch or NULL arrays");
+    if ((with_j && !vj) || (with_k && !vk)) return fail(JK_ERR_ARG, "jk_batch_build: output is NULL");
+    Engine &E = batch->eng;
+    DeviceGuard g(E.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<Item> items(nplans);
+    for (int i = 0; i < nplans; ++i) {
+        items[i].p = plans[i];
+        items[i].dm = dms[i];
+        items[i].n_dm = n_dm[i];
+        items[i].vj = with_j ? vj[i] : nullptr;
+        items[i].vk = with_k ? vk[i] : nullptr;
+    }
+    const Spec s{hermi, with_j, with_k, mixed_threshold};
+    batch->last_replayed = batch->last_captured = 0;
+    if (!use_graph || !batch->warmed) {
+        RC(engine_build(E, items, s, st, nullptr, 0, false, "jk_batch_build"));
+        batch->warmed = true;
+        return JK_OK;
+    }
+    RC(engine_prepare(E, items, s, nullptr, 0, false, "jk_batch_build"));
+    const int spec[4] = {hermi, with_j, with_k, E.shard_rank * 65536 + E.shard_size};
+    const bool same = batch->gexec && E.blob == batch->graph_blob && E.blob_dev == batch->graph_blob &&
+                      batch->graph_alloc_gen == E.alloc_gen && batch->graph_tune_gen == E.tune_gen &&
+                      std::memcmp(spec, batch->graph_spec, sizeof(spec)) == 0 &&
+                      batch->graph_mixed == mixed_threshold;
+    RC(engine_upload(E, st));
+    if (!same) {
+        if (batch->gexec) {
+            cudaGraphExecDestroy(batch->gexec);
+            batch->gexec = nullptr;
+        }
+        RC(engine_configure(E));
+        CK(cudaStreamBeginCapture(batch->cap_stream, cudaStreamCaptureModeRelaxed));
+        const int rc = engine_launch(E, batch->cap_stream, false);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(batch->cap_stream, &graph);
+        if (rc != JK_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        CK(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&batch->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(ie);
+        batch->graph_blob = E.blob;
+        batch->graph_alloc_gen = E.alloc_gen;
+        batch->graph_tune_gen = E.tune_gen;
+        std::memcpy(batch->graph_spec, spec, sizeof(spec));
+        batch->graph_mixed = mixed_threshold;
+        batch->graph_launches = E.launches;
+        batch->last_captured = 1;
+    } else {
+        batch->last_replayed = 1;
+    }
+    CK(cudaGraphLaunch(batch->gexec, st));
+    E.launches = batch->graph_launches;
+    if (E.timing) std::fill(E.ev_used.begin(), E.ev_used.end(), 0);
+    return engine_finish(E, st);
+}
+
+extern "C" int jk_batch_sync(jk_batch *batch, void *stream)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_sync: batch is NULL");
+    DeviceGuard g(batch->eng.device);
+    return engine_sync(batch->eng, (cudaStream_t)stream, "jk_batch_sync");
+}
+
+extern "C" int jk_batch_counts(jk_batch *batch, unsigned long long *quartets,
+                               unsigned long long *prim_quartets,
+                               unsigned long long *quartets_f32, int ncounts, int *nclasses)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_counts: batch is NULL");
+    DeviceGuard g(batch->eng.device);
+    return engine_counts(batch->eng, quartets, prim_quartets, quartets_f32, ncounts, nclasses);
+}
+
+extern "C" int jk_batch_set_timing(jk_batch *batch, int enable)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_set_timing: batch is NULL");
+    DeviceGuard g(batch->eng.device);
+    return engine_set_timing(batch->eng, enable);
+}
+
+extern "C" int jk_batch_class_ms(jk_batch *batch, float *ms, int ncounts, int *launches)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_class_ms: batch is NULL");
+    DeviceGuard g(batch->eng.device);
+    return engine_class_ms(batch->eng, ms, ncounts, launches);
+}
+
+extern "C" int jk_batch_set_tuning(jk_batch *batch, int cls, int tasks_per_sm, int blocks_per_sm)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_set_tuning: batch is NULL");
+    return engine_set_tuning(batch->eng, cls, tasks_per_sm, blocks_per_sm);
+}
+
+extern "C" int jk_batch_stats(jk_batch *batch, int *graph_replayed, int *graph_captured,
+                              long long *workspace_bytes)
+{
+    if (!batch) return fail(JK_ERR_ARG, "jk_batch_stats: batch is NULL");
+    if (graph_replayed) *graph_replayed = batch->last_replayed;
+    if (graph_captured) *graph_captured = batch->last_captured;
+    if (workspace_bytes)
+        *workspace_bytes = (long long)(batch->eng.ws_size + batch->eng.blob_cap +
+                                       4 * (size_t)batch->eng.max_rows * sizeof(int));
+    return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// class table and measurement helpers
+// ---------------------------------------------------------------------------
 extern "C" int jk_class_info(int k, int *li, int *lj, int *lk, int *ll, int *form)
 {
     if (k < 0 || k >= JK_NCLASSES) return fail(JK_ERR_ARG, "jk_class_info: no such class");
@@ -696,34 +1400,6 @@ extern "C" int jk_class_info(int k, int *li, int *lj, int *lk, int *ll, int *for
     if (lk) *lk = c.lk;
     if (ll) *ll = c.ll;
     if (form) *form = c.form;
-    return JK_OK;
-}
-
-extern "C" int jk_set_timing(jk_plan *plan, int enable)
-{
-    if (!plan) return fail(JK_ERR_ARG, "jk_set_timing: plan is NULL");
-    DeviceGuard g(plan->device);
-    if (enable && plan->ev.empty()) {
-        plan->ev.resize(2 * JK_NCLASSES);
-        for (auto &e : plan->ev) CK(cudaEventCreate(&e));
-        plan->ev_used.assign(JK_NCLASSES, 0);
-    }
-    plan->timing = enable != 0;
-    return JK_OK;
-}
-
-extern "C" int jk_last_class_ms(jk_plan *plan, float *ms, int ncounts, int *launches)
-{
-    if (!plan) return fail(JK_ERR_ARG, "jk_last_class_ms: plan is NULL");
-    DeviceGuard g(plan->device);
-    if (launches) *launches = plan->launches;
-    if (!ms) return JK_OK;
-    CK(cudaStreamSynchronize(plan->last_stream));
-    for (int c = 0; c < ncounts && c < JK_NCLASSES; ++c) {
-        ms[c] = 0.f;
-        if (plan->timing && c < (int)plan->ev_used.size() && plan->ev_used[c])
-            CK(cudaEventElapsedTime(&ms[c], plan->ev[2 * c], plan->ev[2 * c + 1]));
-    }
     return JK_OK;
 }
 

@@ -1,10 +1,11 @@
 // Device-side data layout and helpers of the B200 J/K engine.
 //
 // Layout in HBM (all arrays owned by a plan, see jk_api.cu):
-//   prim-pair records  double[8] per kept primitive pair
-//                      {a_ij, K_ij, Px, Py, Pz, PAx, PAy, PAz}
+//   prim-pair records  double[JK_PRIM_STRIDE] per kept primitive pair
+//                      {a_ij, 1/(2 a_ij), Kp_ij, Px, Py, Pz, PAx, PAy, PAz, 0}
 //                      a_ij = a_i + a_j, K_ij = c_i c_j exp(-a_i a_j/a_ij |AB|^2)
 //                      (c with libcint's s/p angular factor folded in),
+//                      Kp_ij = sqrt(2 pi^(5/2)) K_ij / a_ij,
 //                      P the product centre, PA = P - A.
 //   shell-pair records PairRec per shell pair, grouped by pair class
 //                      (la, lb), la >= lb, each group sorted by q descending.
@@ -36,42 +37,50 @@ struct PairRec {
     double ABx, ABy, ABz;  // A - B, for the i -> j transfer
 };
 
-struct ClassArgs {
-    const PairRec *bra;      // bra pair class, sorted by q desc
-    const PairRec *ket;      // ket pair class, sorted by q desc
-    int nbra, nket;
-    int same_class;          // bra and ket are the same pair class
-    int max_bra_prim;        // largest primitive-pair count of a bra pair
-    const double *prim;      // prim-pair records (8 doubles each)
-    const double *rys;       // Rys table (double): Chebyshev part + large-x
-    const float *rys32;      // Rys table (float)
+// One plan (molecule) as one class launch sees it.  A launch covers a list
+// of views -- one plan for an ordinary build, hundreds in a batched build --
+// and every task names the view it belongs to.
+struct PlanView {
+    const PairRec *bra;      // bra pair class of this plan (sub-lists, q desc)
+    const PairRec *ket;      // ket pair class of this plan
+    const int2 *sub;         // ket sub-lists [begin, end) within the ket class
+    const double *prim;      // prim-pair records of this plan
     const float *dm_cond;    // nbas x nbas
-    int nbas;
-    float log_tol;
     const float *dm_max;     // device scalar: max of dm_cond
-    int nao;
     // K densities: dmK[0..n_ka) then dmKT[0..n_k-n_ka) (the transposes, for
     // non-hermitian builds).  J reads dsJ[0..n_j) = D + D^T.
     const double *dmK;
     const double *dmKT;
-    int n_ka, n_k;
     const double *dsJ;
-    int n_j;
     double *Kh;              // half-K accumulators (n_k, nao, nao)
     double *Jh;              // half-J accumulators (n_j, nao, nao)
+    int nbra, nket, nsub, same_class;
+    int nbas, nao, n_ka, n_k;
+    int n_j;
+    float log_tol;
+    float mixed_log_thr;     // mixed precision: quartets whose screened
+                             // bound is below this run in FP32 (-inf: off)
+    int row0;                // first task row of this view in the launch
+};
+
+struct ClassArgs {
+    PlanView v0;             // the view of a single-view launch (by value: it
+                             // is read from the kernel parameters)
+    const PlanView *views;
+    const int *view_row0;    // first task row of each view (binary search)
+    int nviews;
+    int nrows;
+    int max_bra_prim;        // largest primitive-pair count of a bra pair
+    int shard_rank, shard_size;   // this GPU takes tasks t = rank mod size
+    const double *rys;       // Rys table (double): polynomial part + large-x
+    const float *rys32;      // Rys table (float)
     int *counter;            // task counter for the persistent grid
-    // task decomposition: rows r = bra * nsub + sub-list
-    const int2 *sub;         // ket sub-lists [begin, end) within the ket class
-    int nsub;
     const int *chunk;        // kets per task (device scalar, set per launch)
     const int *row_ncand;    // candidate kets per row
     const int *row_prefix;   // inclusive prefix sum of chunks per row
     unsigned long long *nquartets;  // quartets evaluated (statistics)
     unsigned long long *nprimq;     // primitive quartets evaluated
     unsigned long long *nquartets32;  // quartets evaluated in FP32
-    float mixed_log_thr;     // mixed precision: quartets whose screened
-                             // bound is below this run in FP32 (-inf: off)
-    int *error;              // device error flag
 };
 
 // ---------------------------------------------------------------------------

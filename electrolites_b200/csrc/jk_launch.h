@@ -4,11 +4,14 @@
 #include <cuda_runtime.h>
 #include "jk_device.cuh"
 
+#define JK_MAX_DEVICES 64
+
 struct LaunchCfg {
     cudaStream_t stream;
+    int device;            // current device ordinal (< JK_MAX_DEVICES)
     int num_sms;
-    int blocks_per_sm;     // persistent grid: num_sms * blocks_per_sm blocks
-    int mixed;             // 1: mixed-precision instantiation
+    int blocks_per_sm;     // cap on resident blocks per SM (0: occupancy limit)
+    int configure_only;    // 1: set the kernel's attributes, launch nothing
     char *msg;             // 256 bytes: launch failure details
 };
 

@@ -162,114 +162,162 @@ __global__ void schwarz_kernel(const int4 *__restrict__ pairs, int npairs,
 }
 
 // ---------------------------------------------------------------------------
-// dm_cond[ish][jsh] = log max |D[d][a][b]|, |D[d][b][a]| over densities and
-// the shells' AOs (symmetric by construction); and its maximum.
+// Density preparation and J/K assembly over every item of a build (one plan
+// and its densities per item; a single build is a batch of one).  Each
+// launch walks a list of descriptors; a block finds its descriptor by a
+// binary search over the descriptors' first block.
 // ---------------------------------------------------------------------------
-__global__ void dm_cond_kernel(const double *__restrict__ dm, int n_dm, int nao,
-                               const int *__restrict__ sh_ao, const int *__restrict__ sh_nf,
-                               int nbas, float *__restrict__ dm_cond)
+
+// out[d] = a[d] + f * b[d]^T and outT[d] = b[d]^T for d < nd, n x n
+// matrices in 32 x 32 tiles.  A NULL a or b reads as zero; a NULL out or
+// outT is not written.  Used with a = b = D for D + D^T (+ D^T) and with the
+// half-J/K accumulators for the final J/K.
+struct TileOp {
+    const double *a;
+    const double *b;
+    double *out;
+    double *outT;
+    double f;
+    int n, nd;
+    int nt;             // tiles per side, ceil(n / 32)
+    long long tile0;    // first block of this op in the launch
+};
+
+__global__ void tile_op_kernel(const TileOp *__restrict__ ops, int nops)
 {
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double tile[32][33];
+    const long long t = blockIdx.x;
+    int lo = 0, hi = nops - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ops[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+    }
+    const TileOp o = ops[lo];
+    long long r = t - o.tile0;
+    const long long per = (long long)o.nt * o.nt;
+    const int d = (int)(r / per);
+    r -= d * per;
+    const int n = o.n;
+    const size_t n2 = (size_t)n * n;
+    const int bx = (int)(r / o.nt) * 32, by = (int)(r % o.nt) * 32;
+    const double *y = o.b ? o.b + d * n2 : nullptr;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int rr = bx + k, c = by + threadIdx.x;     // b[rr][c], coalesced
+        tile[k][threadIdx.x] = (y && rr < n && c < n) ? y[(size_t)rr * n + c] : 0.;
+    }
+    __syncthreads();
+    const double *x = o.a ? o.a + d * n2 : nullptr;
+    double *out = o.out ? o.out + d * n2 : nullptr;
+    double *outT = o.outT ? o.outT + d * n2 : nullptr;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int rr = by + k, c = bx + threadIdx.x;     // (b^T)[rr][c] = tile[tx][k]
+        if (rr < n && c < n) {
+            const double bt = tile[threadIdx.x][k];
+            const size_t idx = (size_t)rr * n + c;
+            if (out) out[idx] = (x ? x[idx] : 0.) + o.f * bt;
+            if (outT) outT[idx] = bt;
+        }
+    }
+}
+
+// Density screening table of one item:
+// dm_cond[ish][jsh] = log max |D[d][a][b]|, |D[d][b][a]| over its densities
+// and the shells' AOs (symmetric by construction), its maximum dm_max, and
+// the range check against the pairs the plan dropped.
+struct CondItem {
+    const double *dm;
+    const int *sh_ao;
+    const int *sh_nf;
+    float *dmc;
+    float *dm_max;
+    int n_dm, nao, nbas;
+    int nt;             // 16 x 16 shell tiles per side
+    long long blk0;     // first block of this item in the launch
+    float q_drop;       // largest Schwarz bound of a pair the plan dropped
+    float q_max;        // largest Schwarz bound of the plan
+    float log_tol;
+    int pad;
+};
+
+__global__ void dm_cond_kernel(const CondItem *__restrict__ items, int nitems)
+{
+    const long long t = blockIdx.x;
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].blk0 <= t) lo = mid; else hi = mid - 1;
+    }
+    const CondItem it = items[lo];
+    const int r = (int)(t - it.blk0);
+    const int i = (r / it.nt) * 16 + threadIdx.y;
+    const int j = (r % it.nt) * 16 + threadIdx.x;
+    const int nbas = it.nbas, nao = it.nao;
     if (i >= nbas || j >= nbas) return;
-    const int a0 = sh_ao[i], na = sh_nf[i], b0 = sh_ao[j], nb = sh_nf[j];
+    const int a0 = __ldg(it.sh_ao + i), na = __ldg(it.sh_nf + i);
+    const int b0 = __ldg(it.sh_ao + j), nb = __ldg(it.sh_nf + j);
     const size_t nao2 = (size_t)nao * nao;
     double m = 0.;
-    for (int d = 0; d < n_dm; ++d) {
-        const double *D = dm + d * nao2;
+    for (int d = 0; d < it.n_dm; ++d) {
+        const double *D = it.dm + d * nao2;
         for (int a = 0; a < na; ++a)
             for (int b = 0; b < nb; ++b) {
                 m = fmax(m, fabs(D[(size_t)(a0 + a) * nao + b0 + b]));
                 m = fmax(m, fabs(D[(size_t)(b0 + b) * nao + a0 + a]));
             }
     }
-    dm_cond[(size_t)i * nbas + j] = m > 0. ? (float)log(m) : -INFINITY;
+    it.dmc[(size_t)i * nbas + j] = m > 0. ? (float)log(m) : -INFINITY;
 }
 
-__global__ void max_reduce_kernel(const float *__restrict__ v, long long n, float *__restrict__ out)
+// one block per item: dm_max, and err = {JK_ERR_RANGE, item} if a pair the
+// plan dropped could pass the screening with this density
+// (q_drop + q_max + dm_max > log_tol)
+__global__ void dm_max_kernel(const CondItem *__restrict__ items, int *__restrict__ err)
 {
-    __shared__ float s[1024];
+    __shared__ float s[256];
+    const CondItem it = items[blockIdx.x];
+    const long long n = (long long)it.nbas * it.nbas;
     float m = -INFINITY;
-    for (long long k = threadIdx.x; k < n; k += blockDim.x) m = fmaxf(m, v[k]);
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) m = fmaxf(m, it.dmc[k]);
     s[threadIdx.x] = m;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) s[threadIdx.x] = fmaxf(s[threadIdx.x], s[threadIdx.x + w]);
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out = s[0];
-}
-
-// error if a pair dropped at plan time could pass the screening with this
-// density: q_drop + q_max + dm_max > log_tol
-__global__ void range_check_kernel(const float *__restrict__ dm_max, float q_drop, float q_max,
-                                   float log_tol, int *__restrict__ err)
-{
-    if (q_drop + q_max + *dm_max > log_tol) atomicCAS(err, 0, 5);
-}
-
-// out[d] = X[d] + sign * Y[d]^T, 32x32 tiles (also used with Y = X)
-__global__ void add_transpose_kernel(const double *__restrict__ X, const double *__restrict__ Y,
-                                     double sign, int nao, double *__restrict__ out)
-{
-    __shared__ double tile[32][33];
-    const size_t nao2 = (size_t)nao * nao;
-    const int d = blockIdx.z;
-    const double *x = X + d * nao2;
-    const double *y = Y + d * nao2;
-    double *o = out + d * nao2;
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        const int r = bx + k, c = by + threadIdx.x;   // read Y[r][c] coalesced
-        tile[k][threadIdx.x] = (r < nao && c < nao) ? y[(size_t)r * nao + c] : 0.;
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        const int r = by + k, c = bx + threadIdx.x;   // out[r][c] += sign * Y[c][r]
-        if (r < nao && c < nao)
-            o[(size_t)r * nao + c] = x[(size_t)r * nao + c] + sign * tile[threadIdx.x][k];
+    if (threadIdx.x == 0) {
+        *it.dm_max = s[0];
+        if (it.q_drop + it.q_max + s[0] > it.log_tol && atomicCAS(err, 0, 5) == 0)
+            err[1] = blockIdx.x;
     }
 }
 
-// out[d] = D[d]^T
-__global__ void transpose_kernel(const double *__restrict__ D, int nao, double *__restrict__ out)
-{
-    __shared__ double tile[32][33];
-    const size_t nao2 = (size_t)nao * nao;
-    const int d = blockIdx.z;
-    const double *x = D + d * nao2;
-    double *o = out + d * nao2;
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        const int r = bx + k, c = by + threadIdx.x;
-        tile[k][threadIdx.x] = (r < nao && c < nao) ? x[(size_t)r * nao + c] : 0.;
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        const int r = by + k, c = bx + threadIdx.x;
-        if (r < nao && c < nao) o[(size_t)r * nao + c] = tile[threadIdx.x][k];
-    }
-}
-
-// Rows of the task decomposition: one per (bra pair b, ket sub-list s),
-// r = b * nsub + s.  row_ncand[r] = kets of sub-list s (sorted by q) that can
-// pass the Schwarz test with the largest density element, limited to ket
-// index <= b within a diagonal class.
-__global__ void task_rows_kernel(const ClassArgs a)
+// Rows of the task decomposition: one per (view v, bra pair b, ket sub-list
+// s), r = row0(v) + b * nsub(v) + s.  row_ncand[r] = kets of sub-list s
+// (sorted by q) that can pass the Schwarz test with the plan's largest
+// density element, limited to ket index <= b within a diagonal class.
+__global__ void task_rows_kernel(const ClassArgs a, int *__restrict__ row_ncand)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nbra * a.nsub) return;
-    const int b = r / a.nsub, s = r - (r / a.nsub) * a.nsub;
-    const float cut = a.log_tol - a.bra[b].q - *a.dm_max;
-    int lo = a.sub[s].x, hi = a.sub[s].y;
-    if (a.same_class && hi > b + 1) hi = b + 1;
+    if (r >= a.nrows) return;
+    int lo = 0, hi = a.nviews - 1;
+    while (lo < hi) {                    // last view with row0 <= r
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.view_row0[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    const PlanView &V = a.views[lo];
+    const int rl = r - V.row0;
+    const int b = rl / V.nsub, s = rl - (rl / V.nsub) * V.nsub;
+    const float cut = V.log_tol - V.bra[b].q - *V.dm_max;
+    lo = V.sub[s].x;
+    hi = V.sub[s].y;
+    if (V.same_class && hi > b + 1) hi = b + 1;
     const int first = lo;
     if (lo > hi) hi = lo;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (a.ket[mid].q > cut) lo = mid + 1; else hi = mid;
+        if (V.ket[mid].q > cut) lo = mid + 1; else hi = mid;
     }
-    const_cast<int *>(a.row_ncand)[r] = lo - first;
+    row_ncand[r] = lo - first;
 }
 
 // Task size from the class's total candidate count (cand_prefix[rows-1]):

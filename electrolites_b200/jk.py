@@ -209,6 +209,27 @@ class VHFOpt:
                 out[tuple(x.value for x in ls[:4])] = float(ms[k])
         return out, launches.value
 
+    def set_shard(self, rank: int, size: int):
+        """Later builds evaluate only this rank's share of the task lists
+        (tasks rank, rank + size, ...); the sum of vj / vk over the ranks is
+        the full result (electrolites_b200.shard does the all-reduce)."""
+        _lib.check(_lib.lib().jk_plan_set_shard(self.plan, int(rank), int(size)),
+                   'jk_plan_set_shard')
+
+    def set_tuning(self, cls: int, tasks_per_sm: int, blocks_per_sm: int = 0):
+        """Per-class launch tuning (class index k of class_keys(); -1 resets
+        every class)."""
+        _lib.check(_lib.lib().jk_plan_set_tuning(self.plan, int(cls), int(tasks_per_sm),
+                                                 int(blocks_per_sm)), 'jk_plan_set_tuning')
+
+    def memory(self):
+        """(bytes of the plan's resident tables, bytes of its build workspace)."""
+        t = ctypes.c_longlong()
+        w = ctypes.c_longlong()
+        _lib.check(_lib.lib().jk_plan_memory(self.plan, ctypes.byref(t), ctypes.byref(w)),
+                   'jk_plan_memory')
+        return t.value, w.value
+
     def q_cond(self):
         nb = len(self._bas)
         q = np.zeros((nb, nb), dtype=np.float32)
@@ -216,6 +237,19 @@ class VHFOpt:
             self.plan, q.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nb),
             'jk_plan_q_cond')
         return q
+
+
+def class_keys():
+    """[(li, lj, lk, ll), ...] of the engine's classes, by class index."""
+    L = _lib.lib()
+    keys = []
+    k = 0
+    while True:
+        ls = [ctypes.c_int() for _ in range(5)]
+        if L.jk_class_info(k, *[ctypes.byref(x) for x in ls]) != 0:
+            return keys
+        keys.append(tuple(x.value for x in ls[:4]))
+        k += 1
 
 
 def _check_omega(omega):

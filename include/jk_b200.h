@@ -158,6 +158,76 @@ int jk_fp64_peak(int device, double *tflops);
  * general contraction. */
 int jk_plan_q_cond(const jk_plan *plan, float *q_host, int nbas);
 
+/* Device memory the plan holds: its pair tables and task-row buffers, and
+ * the workspace of its own builds (grown on demand and kept). */
+int jk_plan_memory(const jk_plan *plan, long long *table_bytes,
+                   long long *workspace_bytes);
+
+/*
+ * Multi-GPU sharding of a plan's builds: with size > 1 a build evaluates
+ * only the tasks t = rank + size * n of every class's task list, so the
+ * vj / vk it returns are this rank's part and the sum over ranks (an
+ * all-reduce) is the full result.  All ranks must build with the same
+ * plan parameters and densities.  size = 1 (the default) is the whole build.
+ * No counterpart in the reference, which runs on one GPU
+ * (electrolites/fastk.py:657).
+ */
+int jk_plan_set_shard(jk_plan *plan, int rank, int size);
+
+/*
+ * Per-class launch tuning of the plan's builds: the number of tasks per SM
+ * the task size aims at, and a cap on resident blocks per SM (0: the
+ * occupancy limit).  cls = -1 restores the defaults of every class; a 0
+ * tasks_per_sm restores that class's default.  Set by the autotuner
+ * (electrolites_b200/autotune.py); the reference picks its launch shapes in
+ * its code generator (electrolites/codegen/gen_khigh.py).
+ */
+int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_sm);
+
+/*
+ * Batched builds: J/K for many molecules (plans) in one launch stream, each
+ * with its own densities (n_dm[i] of them, dms[i] on the device) and
+ * outputs (vj[i], vk[i]).  Each angular-momentum class runs as one
+ * persistent kernel over the task lists of every plan in the batch.
+ * hermi, with_j, with_k and mixed_threshold apply to every plan and mean
+ * what they mean for jk_build; the results equal those of one jk_build per
+ * plan.  Arrays of pointers are host arrays.
+ *
+ * use_graph = 1: the launch stream is captured in a CUDA graph and replayed
+ * by later calls with the same plans, buffers and parameters (new density
+ * values in the same buffers are fine); the first use_graph call of a batch
+ * runs without capture.  One batch per stream at a time.
+ *
+ * No counterpart in the reference, which builds one molecule per call
+ * (electrolites/fastjk.py:276).
+ */
+typedef struct jk_batch jk_batch;
+int jk_batch_create(int device, jk_batch **out);
+int jk_batch_destroy(jk_batch *batch);
+int jk_batch_build(jk_batch *batch, jk_plan *const *plans, int nplans,
+                   const double *const *dms, const int *n_dm, int hermi,
+                   int with_j, int with_k, double *const *vj, double *const *vk,
+                   double mixed_threshold, int use_graph, void *stream);
+/* Wait for the batch's work on stream; JK_ERR_RANGE names the plan index
+ * whose density is beyond its plan's range. */
+int jk_batch_sync(jk_batch *batch, void *stream);
+/* As jk_last_counts, summed over the plans of the last batched build. */
+int jk_batch_counts(jk_batch *batch, unsigned long long *quartets,
+                    unsigned long long *prim_quartets,
+                    unsigned long long *quartets_f32, int ncounts,
+                    int *nclasses);
+/* As jk_set_timing / jk_last_class_ms (no per-class times for graph
+ * replays). */
+int jk_batch_set_timing(jk_batch *batch, int enable);
+int jk_batch_class_ms(jk_batch *batch, float *ms, int ncounts, int *launches);
+/* As jk_plan_set_tuning, for the batch's builds. */
+int jk_batch_set_tuning(jk_batch *batch, int cls, int tasks_per_sm,
+                        int blocks_per_sm);
+/* Whether the last build replayed or captured a graph, and the batch's
+ * device workspace. */
+int jk_batch_stats(jk_batch *batch, int *graph_replayed, int *graph_captured,
+                   long long *workspace_bytes);
+
 const char *jk_last_error(void);
 
 #ifdef __cplusplus

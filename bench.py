@@ -250,6 +250,32 @@ def run_batch(args, dev, stream, flush, peak_tflops):
     }
 
 
+SERVE_SEED = 20261207
+
+
+def run_serve(args, dev):
+    """Serving: Poisson arrivals of water-cluster requests (3-60 waters,
+    6-31G* or def2-SVP, 1-4 densities, 10 SCF-like cycles with a 1e-4
+    relative density perturbation per cycle), continuous batching over
+    resident plans with admission by an HBM budget (half the device).
+    Plain and mixed forms at each rate; mols/s and latency percentiles."""
+    from electrolites_b200.serve import JKServer, latency_stats, poisson_requests
+    out = {'workload': 'serve_h2o3-60_631gs_svp', 'requests': args.serve_requests,
+           'cycles': 10, 'hbm_budget': 'half of device memory', 'rates': []}
+    for rate in args.serve_rates:
+        row = {'rate_req_per_s': rate}
+        for form, thr in (('plain', 0.0), ('mixed', BATCH_MIXED)):
+            reqs = poisson_requests(args.serve_requests, rate, SERVE_SEED)
+            srv = JKServer(dev.index, hbm_budget=0.5, mixed_threshold=thr)
+            srv.run(reqs)
+            st = latency_stats(reqs)
+            row[form] = {k: round(v, 3) for k, v in st.items()}
+            row[form]['mean_batch'] = round(sum(srv.batch_sizes) / len(srv.batch_sizes), 2)
+            row[form]['iterations'] = srv.iterations
+        out['rates'].append(row)
+    return out
+
+
 def run_ours(args, rank, world):
     import ctypes
 
@@ -362,6 +388,10 @@ def run_ours(args, rank, world):
     if rank == 0 and world == 1 and not args.no_batch:
         batched = run_batch(args, dev, stream, flush, peak_tflops)
 
+    serving = None
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        serving = run_serve(args, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, thr_used, desc = cpu_sample(mol, dms_h, budget_s=args.cpu_budget)
@@ -397,6 +427,7 @@ def run_ours(args, rank, world):
             'clocks': clk,
             'cpu_baseline': cpu,
             'batched': batched,
+            'serving': serving,
         }
         print(json.dumps(line), flush=True)
 
@@ -411,6 +442,10 @@ def main():
     ap.add_argument('--mixed', type=float, default=0.0)
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--serve-requests', type=int, default=32,
+                    help='requests per serving run (0: skip serving)')
+    ap.add_argument('--serve-rates', type=float, nargs='+', default=[200.0],
+                    help='Poisson arrival rates (requests/s) of the serving runs')
     ap.add_argument('--no-batch', action='store_true',
                     help='skip the uneven-batch comparison (plain vs batched vs mixed)')
     args = ap.parse_args()

@@ -1,0 +1,130 @@
+"""Per-class launch tuning of the J/K engine, picked by measurement.
+
+Every class kernel has two runtime knobs (jk_plan_set_tuning /
+jk_batch_set_tuning): the number of tasks per SM its task size aims at --
+more, smaller tasks balance the persistent grid better, fewer, larger ones
+stage fewer bra pairs and claim fewer tasks -- and a cap on resident blocks
+per SM.  The tuner times every candidate setting on a workload, all classes
+at once with per-class CUDA-event times, keeps the fastest setting of each
+class, and stores the table as JSON keyed by device name and form
+('single' for one-molecule builds, 'batch' for batched builds).  Plans and
+batches created later on a device with a stored table start from it.
+
+    python -m electrolites_b200.autotune [--out electrolites_b200/tuning.json]
+
+The reference picks its launch shapes in its code generator
+(electrolites/codegen/gen_khigh.py); here they are measured on the device.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+from .jk import class_keys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE_PATH = os.path.join(HERE, 'tuning.json')
+
+# (tasks per SM, blocks-per-SM cap; 0 = occupancy limit)
+CANDIDATES = [(16, 0), (32, 0), (64, 0), (128, 0), (256, 0), (64, 1)]
+
+
+def _key(k):
+    return ''.join(map(str, k))
+
+
+def tune(target, run, reps: int = 2, candidates=CANDIDATES) -> dict:
+    """target: a VHFOpt or JKBatch; run(): one synchronised build on it,
+    without graph replay (per-class times come from its events).
+    Returns {class key: [tasks_per_sm, blocks_per_sm]} and applies it."""
+    keys = class_keys()
+    target.set_timing(True)
+    best = {}
+    for cand in candidates:
+        for i in range(len(keys)):
+            target.set_tuning(i, *cand)
+        run()
+        tot = {}
+        for _ in range(reps):
+            run()
+            ms, _ = target.last_class_ms()
+            for k, v in ms.items():
+                tot[k] = tot.get(k, 0.0) + v / reps
+        for k, v in tot.items():
+            if k not in best or v < best[k][0]:
+                best[k] = (v, cand)
+    target.set_tuning(-1, 0, 0)
+    table = {_key(k): list(c) for k, (_, c) in best.items()}
+    apply(target, table)
+    return table
+
+
+def apply(target, table: dict):
+    """Set a stored table on a VHFOpt or JKBatch (classes absent from the
+    table keep their defaults)."""
+    for i, k in enumerate(class_keys()):
+        c = table.get(_key(k))
+        if c is not None:
+            target.set_tuning(i, int(c[0]), int(c[1]))
+
+
+def device_name(device: int) -> str:
+    import torch
+    return torch.cuda.get_device_name(device)
+
+
+def load(device: int, form: str, path: str = TABLE_PATH):
+    """The stored table of this device and form, or None."""
+    try:
+        with open(path) as f:
+            data = json.load(f)
+    except (OSError, ValueError):
+        return None
+    return data.get(device_name(device), {}).get(form)
+
+
+def save(device: int, form: str, table: dict, workload: str, path: str = TABLE_PATH):
+    data = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+    entry = data.setdefault(device_name(device), {})
+    entry[form] = table
+    entry.setdefault('workloads', {})[form] = workload
+    with open(path, 'w') as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+
+
+def main():
+    import torch
+
+    from . import clusters
+    from .batch import JKBatch
+    from .jk import VHFOpt
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--out', default=TABLE_PATH)
+    ap.add_argument('--reps', type=int, default=2)
+    ap.add_argument('--batch-mols', type=int, default=512)
+    args = ap.parse_args()
+    dev = torch.device('cuda', torch.cuda.current_device())
+    # single: (H2O)_96, 6-31G*, UHF pair
+    mol = clusters.water_mole(96, 15.0, 20261204)
+    dms = torch.as_tensor(clusters.uhf_pair(clusters.atomic_density(mol, 20261204), 20261205),
+                          device=dev)
+    opt = VHFOpt(mol, 1e-13).build()
+    table = tune(opt, lambda: opt.get_jk(dms, 1), args.reps)
+    save(dev.index, 'single', table, '(H2O)96 6-31G* UHF pair', args.out)
+    print('single', json.dumps(table))
+    # batch: uneven 1-24 water clusters, 6-31G*, 1-4 densities
+    items = clusters.uneven_batch(args.batch_mols, 20261206)
+    opts = [VHFOpt(m, 1e-13).build() for m, _ in items]
+    bd = [torch.as_tensor(d, device=dev) for _, d in items]
+    batch = JKBatch(dev.index)
+    table = tune(batch, lambda: batch.build(opts, bd, 1), args.reps)
+    save(dev.index, 'batch', table, f'{args.batch_mols} water clusters 1-24, 6-31G*', args.out)
+    print('batch', json.dumps(table))
+
+
+if __name__ == '__main__':
+    main()

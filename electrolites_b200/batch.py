@@ -40,6 +40,10 @@ class JKBatch:
         _lib.check(_lib.lib().jk_batch_create(self.device, ctypes.byref(h)), 'jk_batch_create')
         self._h = h
         self._keep = None
+        from . import autotune
+        table = autotune.load(self.device, 'batch')
+        if table:
+            autotune.apply(self, table)
 
     def __del__(self):
         try:

@@ -371,7 +371,8 @@ def write_all(outdir, lmax=LMAX):
            '#pragma once',
            '#include "../jk_launch.h"']
     for A, B, cls in classes:
-        reg.append(f'int jk_launch_{cls.tag}(const ClassArgs &a, const LaunchCfg &cfg);')
+        reg.append(f'int jk_launch_{cls.tag}(const ClassArgs &a, const PlanView *views, '
+                   'const LaunchCfg &cfg);')
     reg.append(f'#define JK_NCLASSES {len(classes)}')
     reg.append('static const ClassEntry jk_class_table[JK_NCLASSES] = {')
     for A, B, cls in classes:

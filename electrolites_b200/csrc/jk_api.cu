@@ -137,7 +137,8 @@ struct Engine {
     void *d_cub = nullptr;
     size_t cub_bytes = 0;
     int *d_chunk = nullptr;         // task size per class
-    int *d_counters = nullptr;      // task counter per class
+    int *d_counters = nullptr;      // task counter per class launch
+    int counter_cap = 0;
     unsigned long long *d_nq = nullptr;   // quartets, primitive quartets, FP32 quartets per class
     int *d_error = nullptr;         // {code, item}
     char *h_blob = nullptr;         // pinned staging copy of the descriptors
@@ -164,8 +165,11 @@ struct Engine {
     const float *rys32 = nullptr;
     // layout of the prepared build
     int nitems = 0;
+    int mixed = 0;                  // the build has a mixed-precision threshold
     int cls_view0[JK_NCLASSES], cls_nview[JK_NCLASSES], cls_rows[JK_NCLASSES],
         cls_maxprim[JK_NCLASSES];
+    int cls_nlaunch[JK_NCLASSES], cls_cnt0[JK_NCLASSES];   // launches per class, first counter
+    int ncounters = 0;
     size_t off_views = 0, off_row0 = 0, off_pre = 0, off_post = 0, off_cond = 0;
     int npre = 0, npost = 0;
     long long pre_tiles = 0, post_tiles = 0, cond_blocks = 0;
@@ -234,6 +238,7 @@ static int engine_init(Engine &E, int device)
     RC(rys_tables(device, &E.rys, &E.rys32));
     CK(cudaMalloc(&E.d_chunk, JK_NCLASSES * sizeof(int)));
     CK(cudaMalloc(&E.d_counters, JK_NCLASSES * sizeof(int)));
+    E.counter_cap = JK_NCLASSES;
     CK(cudaMalloc(&E.d_nq, 3 * JK_NCLASSES * sizeof(unsigned long long)));
     CK(cudaMemset(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long)));
     CK(cudaMalloc(&E.d_error, 2 * sizeof(int)));
@@ -439,6 +444,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
 
     // ---- class views ----
     const float log_mixed = s.mixed_threshold > 0 ? (float)std::log(s.mixed_threshold) : -INFINITY;
+    E.mixed = s.mixed_threshold > 0;
     bool any = false;
     for (const Item &it : items) any = any || it.n_j || it.n_k;
     std::vector<PlanView> views;
@@ -491,6 +497,27 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         E.cls_rows[c] = (int)rows;
         E.cls_maxprim[c] = maxprim;
         max_rows = std::max(max_rows, rows);
+    }
+    // launches per class: JK_VTAB views each, every launch with its counter
+    int ncounters = 0;
+    for (int c = 0; c < JK_NCLASSES; ++c) {
+        E.cls_nlaunch[c] = (E.cls_nview[c] + JK_VTAB - 1) / JK_VTAB;
+        E.cls_cnt0[c] = ncounters;
+        ncounters += E.cls_nlaunch[c];
+    }
+    E.ncounters = ncounters;
+    if (ncounters > E.counter_cap) {
+        if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": counters beyond reservation");
+        RC(engine_idle(E));
+        cudaFree(E.d_counters);
+        E.d_counters = nullptr;
+        E.counter_cap = 0;
+        E.alloc_gen++;
+        if (cudaMalloc(&E.d_counters, ncounters * sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(JK_ERR_NOMEM, std::string(who) + ": cannot allocate the task counters");
+        }
+        E.counter_cap = ncounters;
     }
     // ---- density preparation, screening and assembly descriptors ----
     std::vector<TileOp> pre, post;
@@ -586,30 +613,33 @@ static int engine_upload(Engine &E, cudaStream_t st)
     return JK_OK;
 }
 
-static ClassArgs class_args(const Engine &E, int c)
+// launch l of class c: views [l JK_VTAB, ...) of the class
+static ClassArgs class_args(const Engine &E, int c, int l, const PlanView **host_views)
 {
+    const PlanView *hv = (const PlanView *)(E.blob.data() + E.off_views) + E.cls_view0[c];
     ClassArgs a;
-    if (E.cls_nview[c] > 0)
-        std::memcpy(&a.v0, E.blob.data() + E.off_views + E.cls_view0[c] * sizeof(PlanView),
-                    sizeof(PlanView));
-    else
-        std::memset(&a.v0, 0, sizeof(PlanView));
     a.views = (const PlanView *)(E.d_blob + E.off_views) + E.cls_view0[c];
     a.view_row0 = (const int *)(E.d_blob + E.off_row0) + E.cls_view0[c];
     a.nviews = E.cls_nview[c];
     a.nrows = E.cls_rows[c];
+    a.view_begin = l * JK_VTAB;
+    a.nvl = std::min(JK_VTAB, a.nviews - a.view_begin);
+    a.row_begin = hv[a.view_begin].row0;
+    a.row_end = a.view_begin + a.nvl < a.nviews ? hv[a.view_begin + a.nvl].row0 : a.nrows;
     a.max_bra_prim = E.cls_maxprim[c];
+    a.mixed = E.mixed;
     a.shard_rank = E.shard_rank;
     a.shard_size = E.shard_size;
     a.rys = E.rys;
     a.rys32 = E.rys32;
-    a.counter = E.d_counters + c;
+    a.counter = E.d_counters + E.cls_cnt0[c] + l;
     a.chunk = E.d_chunk + c;
     a.row_ncand = E.d_rows;
     a.row_prefix = E.d_rows + 2 * E.max_rows;
     a.nquartets = E.d_nq + c;
     a.nprimq = E.d_nq + JK_NCLASSES + c;
     a.nquartets32 = E.d_nq + 2 * JK_NCLASSES + c;
+    *host_views = hv + a.view_begin;
     return a;
 }
 
@@ -627,9 +657,12 @@ static int engine_configure(Engine &E)
     cfg.msg = msg;
     std::lock_guard<std::mutex> lock(g_launch_mutex);
     for (int c = 0; c < JK_NCLASSES; ++c) {
-        if (!E.cls_nview[c]) continue;
-        const int rc = jk_class_table[c].launch(class_args(E, c), cfg);
-        if (rc) return fail(JK_ERR_CUDA, std::string("class kernel configuration failed: ") + msg);
+        for (int l = 0; l < E.cls_nlaunch[c]; ++l) {
+            const PlanView *hv = nullptr;
+            const ClassArgs a = class_args(E, c, l, &hv);
+            const int rc = jk_class_table[c].launch(a, hv, cfg);
+            if (rc) return fail(JK_ERR_CUDA, std::string("class kernel configuration failed: ") + msg);
+        }
     }
     return JK_OK;
 }
@@ -654,7 +687,7 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
     dm_max_kernel<<<E.nitems, 256, 0, st>>>(d_cond, E.d_error);
     CK(cudaGetLastError());
     E.launches += 2;
-    CK(cudaMemsetAsync(E.d_counters, 0, JK_NCLASSES * sizeof(int), st));
+    if (E.ncounters) CK(cudaMemsetAsync(E.d_counters, 0, E.ncounters * sizeof(int), st));
     CK(cudaMemsetAsync(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
     char msg[256] = {0};
     LaunchCfg cfg;
@@ -670,7 +703,8 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
         const int rows = E.cls_rows[c];
         if (!E.cls_nview[c] || rows == 0) continue;
         const ClassEntry &ce = jk_class_table[c];
-        const ClassArgs a = class_args(E, c);
+        const PlanView *hv = nullptr;
+        const ClassArgs a = class_args(E, c, 0, &hv);
         if (timing) CK(cudaEventRecord(E.ev[2 * c], st));
         // task list: candidates per row, a task size giving about
         // tasks_per_sm tasks per SM, chunks per row, prefix sum of chunks
@@ -687,15 +721,18 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
         CK(cub::DeviceScan::InclusiveSum(E.d_cub, tmp, chunks, prefix, rows, st));
         E.launches += 4;
         cfg.blocks_per_sm = E.tune[c].blocks_per_sm;
-        int rc;
-        {
-            std::lock_guard<std::mutex> lock(g_launch_mutex);
-            rc = ce.launch(a, cfg);
+        for (int l = 0; l < E.cls_nlaunch[c]; ++l) {
+            const ClassArgs al = class_args(E, c, l, &hv);
+            int rc;
+            {
+                std::lock_guard<std::mutex> lock(g_launch_mutex);
+                rc = ce.launch(al, hv, cfg);
+            }
+            if (rc != 0)
+                return fail(JK_ERR_CUDA, std::string("class kernel launch failed: ") + msg + " " +
+                                             cudaGetErrorString((cudaError_t)rc));
+            E.launches++;
         }
-        if (rc != 0)
-            return fail(JK_ERR_CUDA, std::string("class kernel launch failed: ") + msg + " " +
-                                         cudaGetErrorString((cudaError_t)rc));
-        E.launches++;
         if (timing) {
             CK(cudaEventRecord(E.ev[2 * c + 1], st));
             E.ev_used[c] = 1;

@@ -64,17 +64,19 @@ struct PlanView {
 };
 
 struct ClassArgs {
-    PlanView v0;             // the view of a single-view launch (by value: it
-                             // is read from the kernel parameters)
-    const PlanView *views;
+    const PlanView *views;   // every view of the class (global copy)
     const int *view_row0;    // first task row of each view (binary search)
     int nviews;
     int nrows;
+    // the part of the class this launch covers: views [view_begin,
+    // view_begin + nvl), task rows [row_begin, row_end)
+    int view_begin, nvl, row_begin, row_end;
     int max_bra_prim;        // largest primitive-pair count of a bra pair
+    int mixed;               // 1: the build has FP32 quartets (mixed form)
     int shard_rank, shard_size;   // this GPU takes tasks t = rank mod size
     const double *rys;       // Rys table (double): polynomial part + large-x
     const float *rys32;      // Rys table (float)
-    int *counter;            // task counter for the persistent grid
+    int *counter;            // task counter of this launch
     const int *chunk;        // kets per task (device scalar, set per launch)
     const int *row_ncand;    // candidate kets per row
     const int *row_prefix;   // inclusive prefix sum of chunks per row
@@ -82,6 +84,19 @@ struct ClassArgs {
     unsigned long long *nprimq;     // primitive quartets evaluated
     unsigned long long *nquartets32;  // quartets evaluated in FP32
 };
+
+// Views per launch of a batched class: the launch carries its views in its
+// kernel parameters (__grid_constant__, read through the constant cache, so
+// a view field costs no register while it is not in use).  Kernel
+// parameters may hold 32764 bytes.
+#define JK_VTAB 192
+
+template <int NV>
+struct LaunchParams {
+    ClassArgs a;
+    PlanView v[NV];
+};
+static_assert(sizeof(LaunchParams<JK_VTAB>) <= 32000, "kernel parameters hold at most 32764 bytes");
 
 // ---------------------------------------------------------------------------
 // Rys roots and weights from the piecewise Chebyshev table
@@ -167,40 +182,6 @@ __device__ __forceinline__ void rys_roots(double x, const double *__restrict__ t
 #pragma unroll
     for (int row = 0; row < 2 * N; ++row) {
         const double v = rys_poly10(c + row * (RYS_DEGREE + 1) / 2, s, s2, s4, s8);
-        if (row < N) r[row] = v; else w[row - N] = v;
-    }
-}
-
-// Single-precision variant for the mixed-precision form: a degree-7 table on
-// the same intervals, FP32 arithmetic.  Accuracy ~1e-7 relative.
-template <int N>
-__device__ __forceinline__ void rys_roots_f32(float x, const float *__restrict__ tab,
-                                              float *__restrict__ r,
-                                              float *__restrict__ w)
-{
-    static_assert(RYS_DEGREE_F32 == 7, "degree-7 single-precision table");
-    if (x >= (float)RYS_XMAX) {
-        float ix = rsqrtf(x);
-        float inv = ix * ix;
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-            r[i] = __ldg(tab + RYS32_LARGEX_OFF + (N - 1) * RYS_NMAX + i) * inv;
-            w[i] = __ldg(tab + RYS32_LARGEX_OFF + RYS_NMAX * RYS_NMAX + (N - 1) * RYS_NMAX + i) * ix;
-        }
-        return;
-    }
-    int it;
-    float s;
-    rys_locate_f32(x, it, s);
-    const float s2 = s * s, s4 = s2 * s2;
-    const float4 *c = reinterpret_cast<const float4 *>(
-        tab + rys32_offset<N>() + it * (2 * N * (RYS_DEGREE_F32 + 1)));
-#pragma unroll
-    for (int row = 0; row < 2 * N; ++row) {
-        const float4 lo = __ldg(c + 2 * row), hi = __ldg(c + 2 * row + 1);
-        const float p0 = fmaf(lo.y, s, lo.x), p1 = fmaf(lo.w, s, lo.z);
-        const float p2 = fmaf(hi.y, s, hi.x), p3 = fmaf(hi.w, s, hi.z);
-        const float v = fmaf(fmaf(p3, s2, p2), s4, fmaf(p1, s2, p0));
         if (row < N) r[row] = v; else w[row - N] = v;
     }
 }

@@ -15,7 +15,8 @@ struct LaunchCfg {
     char *msg;             // 256 bytes: launch failure details
 };
 
-typedef int (*ClassLauncher)(const ClassArgs &, const LaunchCfg &);
+// a: the launch's part of the class; views: host copies of its a.nvl views
+typedef int (*ClassLauncher)(const ClassArgs &a, const PlanView *views, const LaunchCfg &cfg);
 
 struct ClassEntry {
     int bra_class, ket_class;     // pair-class indices la*(la+1)/2 + lb

@@ -81,6 +81,10 @@ class VHFOpt:
                    'jk_plan_info')
         self.nao = nao.value
         self.npairs = npairs.value
+        from . import autotune
+        table = autotune.load(self.device, 'single')
+        if table:
+            autotune.apply(self, table)
         return self
 
     def __del__(self):

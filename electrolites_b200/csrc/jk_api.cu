@@ -1041,6 +1041,9 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
         p->pc_maxprim[k] = mp;
     }
     p->pc_off[NPAIR_CLASSES] = (int)recs.size();
+    for (int k = 0; k < NPAIR_CLASSES; ++k)   // kernels queue ket indices in 29 bits
+        if (p->pc_off[k + 1] - p->pc_off[k] >= (1 << 29))
+            return fail(JK_ERR_ARG, "molecule too large (shell pairs of one class)");
     p->sub_off[NPAIR_CLASSES] = (int)p->subs.size();
     CK(upload(&p->d_subs, p->subs, st, &p->table_bytes));
     // task rows of one class: the largest (bra class pairs) x (ket class sub-lists)

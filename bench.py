@@ -41,6 +41,7 @@ WORKLOADS = {
     'h2o8_631gs': (8, 7.0, '6-31g*', False, 20261203),
     'h2o32_631gs_uhf': (32, 10.4, '6-31g*', True, 20261204),
     'h2o64_tzvp': (64, 12.5, 'def2-tzvp', False, 20261205),
+    'h2o16_tzvp': (16, 7.8, 'def2-tzvp', False, 20261205),
 }
 DEFAULT = 'h2o96_631gs_uhf'
 TOL = 1e-13

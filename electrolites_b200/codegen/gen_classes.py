@@ -238,8 +238,9 @@ def gen_row_acc(cls, f0, f1):
 
 
 def gen_hrr(la, lb, prefix, vec):
-    """(a, b) from levels la..la+lb of the input: out[a*nb + b] for a at
-    level la, b at level lb.  in[] is ordered level by level."""
+    """(a, b) from levels la..la+lb of the input: out[(a*nb + b) * SO] for a
+    at level la, b at level lb.  in[k * SI] is ordered level by level (SI, SO:
+    strides, 1 for register arrays, NF for a column of a shared-memory block)."""
     em = Emitter('    ')
     off = {}
     o = 0
@@ -254,7 +255,7 @@ def gen_hrr(la, lb, prefix, vec):
         if key in memo:
             return memo[key]
         if k == 0:
-            expr = f'in[{off[L] + cidx(L, a)}]'
+            expr = f'in[{off[L] + cidx(L, a)} * SI]'
             memo[key] = expr
             return expr
         # recurse on the first nonzero direction of b
@@ -276,7 +277,7 @@ def gen_hrr(la, lb, prefix, vec):
     outs = []
     for ia, a in enumerate(comps(la)):
         for ib, b in enumerate(comps(lb)):
-            outs.append(f'out[{ia * nb + ib}] = {val(la, a, lb, b)};')
+            outs.append(f'out[{ia * nb + ib} * SO] = {val(la, a, lb, b)};')
     for s in outs:
         em(s)
     return em.text()
@@ -332,10 +333,12 @@ def gen_class_header(cls):
                      'T wz, T *acc) {')
         lines.append(gen_root_acc(cls))
         lines.append('    }')
-    lines.append(f'    {tpl} hrr_bra(const T *in, T *out, T ABx, T ABy, T ABz) {{')
+    tpl_s = ('template <class T, int SI = 1, int SO = 1> __device__ static __forceinline__ '
+             'void')
+    lines.append(f'    {tpl_s} hrr_bra(const T *in, T *out, T ABx, T ABy, T ABz) {{')
     lines.append(gen_hrr(cls.li, cls.lj, 'hb', 'AB'))
     lines.append('    }')
-    lines.append(f'    {tpl} hrr_ket(const T *in, T *out, T CDx, T CDy, T CDz) {{')
+    lines.append(f'    {tpl_s} hrr_ket(const T *in, T *out, T CDx, T CDy, T CDz) {{')
     lines.append(gen_hrr(cls.lk, cls.ll, 'hk', 'CD'))
     lines.append('    }')
     lines.append('};')

@@ -18,8 +18,10 @@ N > 1 ranks (torchrun, one GPU each) the build is sharded: every rank
 evaluates the tasks rank, rank + N, ... of each class launch and one NCCL
 all-reduce of the (vj, vk) buffer completes the build on every rank (strong
 scaling: one build per step for the whole job); timing is the max over
-ranks.  The default run also times the uneven 512-molecule batch (one build
-per molecule vs batched FP64 vs batched mixed) and a serving run.
+ranks.  The default run also reports the plain-vs-mixed threshold sweep
+(1e-10..1e-6) on this workload and on (H2O)_64 def2-TZVP, the uneven
+512-molecule batch (one build per molecule vs batched FP64 vs batched
+mixed) and a serving run.
 """
 from __future__ import annotations
 
@@ -256,6 +258,50 @@ def run_batch(args, dev, stream, flush, peak_tflops):
 
 
 SERVE_SEED = 20261207
+MIXED_SWEEP = (1e-10, 1e-8, 1e-7, 1e-6)
+MIXED_WORKLOADS = ('h2o96_631gs_uhf', 'h2o64_tzvp')
+
+
+def run_mixed(args, dev, stream, flush):
+    """Plain FP64 against the mixed form at each threshold of the sweep, on
+    the (H2O)_96 6-31G* UHF pair and (H2O)_64 def2-TZVP: device ms per build,
+    the fraction of quartets run in FP32, and the J/K energy and largest
+    element errors against the plain build (E_J = 1/2 tr(D J),
+    E_K = -1/4 tr(D K) summed over the densities)."""
+    import torch
+
+    from electrolites_b200.jk import VHFOpt
+    out = {}
+    for w in MIXED_WORKLOADS:
+        mol, dms_h = make_inputs(w)
+        opt = VHFOpt(mol, TOL, device=dev.index).build()
+        dms = torch.as_tensor(dms_h, device=dev)
+        res = {}
+        for thr in (0.0,) + MIXED_SWEEP:
+            vj = torch.empty_like(dms)
+            vk = torch.empty_like(dms)
+            ms = _timed(lambda: opt.build_jk_async(dms, 1, True, True, vj, vk, thr, stream),
+                        2, 1, stream, flush)
+            opt.sync(stream)
+            c = opt.class_counts(with_f32=True)
+            nq = sum(v[0] for v in c.values())
+            n32 = sum(v[2] for v in c.values())
+            ej = float(0.5 * (dms * vj).sum())
+            ek = float(-0.25 * (dms * vk).sum())
+            res[thr] = (ms, n32 / max(1, nq), ej, ek, vj, vk)
+        p = res[0.0]
+        row = {'nao_cart': mol.nao_cart, 'n_dm': int(dms.shape[0]), 'plain_ms': round(p[0], 2),
+               'thresholds': {}}
+        for thr in MIXED_SWEEP:
+            m = res[thr]
+            row['thresholds'][f'{thr:g}'] = {
+                'ms': round(m[0], 2), 'speedup': round(p[0] / m[0], 3),
+                'fp32_quartet_frac': round(m[1], 3),
+                'dE_J': m[2] - p[2], 'dE_K': m[3] - p[3],
+                'max_dJ': float((m[4] - p[4]).abs().max()),
+                'max_dK': float((m[5] - p[5]).abs().max())}
+        out[w] = row
+    return out
 
 
 def run_serve(args, dev):
@@ -407,6 +453,10 @@ def run_ours(args, rank, world):
     # correctness guard on the timed output: symmetric, finite
     assert torch.isfinite(vj).all() and torch.isfinite(vk).all()
 
+    mixed = None
+    if rank == 0 and world == 1 and not args.no_mixed:
+        mixed = run_mixed(args, dev, stream, flush)
+
     batched = None
     if rank == 0 and world == 1 and not args.no_batch:
         batched = run_batch(args, dev, stream, flush, peak_tflops)
@@ -449,6 +499,7 @@ def run_ours(args, rank, world):
             'gpu_launches': launches * args.steps,
             'clocks': clk,
             'cpu_baseline': cpu,
+            'mixed': mixed,
             'batched': batched,
             'serving': serving,
         }
@@ -467,8 +518,10 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--serve-requests', type=int, default=32,
                     help='requests per serving run (0: skip serving)')
-    ap.add_argument('--serve-rates', type=float, nargs='+', default=[200.0],
+    ap.add_argument('--serve-rates', type=float, nargs='+', default=[50.0],
                     help='Poisson arrival rates (requests/s) of the serving runs')
+    ap.add_argument('--no-mixed', action='store_true',
+                    help='skip the plain-vs-mixed threshold sweep')
     ap.add_argument('--no-batch', action='store_true',
                     help='skip the uneven-batch comparison (plain vs batched vs mixed)')
     args = ap.parse_args()

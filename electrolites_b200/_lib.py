@@ -64,7 +64,7 @@ def lib():
     ullp = ctypes.POINTER(ctypes.c_ulonglong)
     L.jk_plan_memory.argtypes = [vp, llp, llp]
     L.jk_plan_set_shard.argtypes = [vp, c_int, c_int]
-    L.jk_plan_set_tuning.argtypes = [vp, c_int, c_int, c_int]
+    L.jk_plan_set_tuning.argtypes = [vp, c_int, c_int, c_int, c_int]
     L.jk_batch_create.argtypes = [c_int, ctypes.POINTER(vp)]
     L.jk_batch_destroy.argtypes = [vp]
     L.jk_batch_build.argtypes = [vp, vp, c_int, vp, vp, c_int, c_int, c_int, vp, vp, c_double,
@@ -73,7 +73,7 @@ def lib():
     L.jk_batch_counts.argtypes = [vp, ullp, ullp, ullp, c_int, ip]
     L.jk_batch_set_timing.argtypes = [vp, c_int]
     L.jk_batch_class_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float), c_int, ip]
-    L.jk_batch_set_tuning.argtypes = [vp, c_int, c_int, c_int]
+    L.jk_batch_set_tuning.argtypes = [vp, c_int, c_int, c_int, c_int]
     L.jk_batch_stats.argtypes = [vp, ip, ip, llp]
     L.jk_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:

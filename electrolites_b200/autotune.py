@@ -1,12 +1,15 @@
 """Per-class launch tuning of the J/K engine, picked by measurement.
 
-Every class kernel has two runtime knobs (jk_plan_set_tuning /
+Every class kernel has three runtime knobs (jk_plan_set_tuning /
 jk_batch_set_tuning): the number of tasks per SM its task size aims at --
 more, smaller tasks balance the persistent grid better, fewer, larger ones
-stage fewer bra pairs and claim fewer tasks -- and a cap on resident blocks
-per SM.  The tuner times every candidate setting on a workload, all classes
-at once with per-class CUDA-event times, keeps the fastest setting of each
-class, and stores the table as JSON keyed by device name and form
+stage fewer bra pairs and claim fewer tasks -- a cap on resident blocks per
+SM, and whether mixed-precision builds run the class's low-bound quartets
+in FP32 (the per-class tuned threshold of the mixed form: a class where FP32
+measures slower keeps FP64).  The tuner times every candidate setting on a
+workload, all classes at once with per-class CUDA-event times, keeps the
+fastest setting of each class, and stores the table as JSON keyed by device
+name and form
 ('single' for one-molecule builds, 'batch' for batched builds).  Plans and
 batches created later on a device with a stored table start from it.
 
@@ -28,34 +31,50 @@ TABLE_PATH = os.path.join(HERE, 'tuning.json')
 
 # (tasks per SM, blocks-per-SM cap; 0 = occupancy limit)
 CANDIDATES = [(16, 0), (32, 0), (64, 0), (128, 0), (256, 0), (64, 1)]
+# threshold of the mixed builds the FP32 choice is measured on
+MIXED_THRESHOLD = 1e-6
 
 
 def _key(k):
     return ''.join(map(str, k))
 
 
-def tune(target, run, reps: int = 2, candidates=CANDIDATES) -> dict:
-    """target: a VHFOpt or JKBatch; run(): one synchronised build on it,
-    without graph replay (per-class times come from its events).
-    Returns {class key: [tasks_per_sm, blocks_per_sm]} and applies it."""
+def _class_ms(target, run, reps):
+    run()
+    tot = {}
+    for _ in range(reps):
+        run()
+        ms, _ = target.last_class_ms()
+        for k, v in ms.items():
+            tot[k] = tot.get(k, 0.0) + v / reps
+    return tot
+
+
+def tune(target, run, run_mixed=None, reps: int = 2, candidates=CANDIDATES) -> dict:
+    """target: a VHFOpt or JKBatch; run(): one synchronised plain build on it
+    and run_mixed(): one mixed build, both without graph replay (per-class
+    times come from its events).  Returns {class key: [tasks_per_sm,
+    blocks_per_sm, fp32]} and applies it."""
     keys = class_keys()
     target.set_timing(True)
     best = {}
     for cand in candidates:
         for i in range(len(keys)):
             target.set_tuning(i, *cand)
-        run()
-        tot = {}
-        for _ in range(reps):
-            run()
-            ms, _ = target.last_class_ms()
-            for k, v in ms.items():
-                tot[k] = tot.get(k, 0.0) + v / reps
-        for k, v in tot.items():
+        for k, v in _class_ms(target, run, reps).items():
             if k not in best or v < best[k][0]:
                 best[k] = (v, cand)
-    target.set_tuning(-1, 0, 0)
-    table = {_key(k): list(c) for k, (_, c) in best.items()}
+    target.set_tuning(-1, 0, 0, -1)
+    table = {_key(k): list(c) + [-1] for k, (_, c) in best.items()}
+    if run_mixed is not None:
+        timed = {}
+        for fp32 in (1, 0):
+            apply(target, {k: v[:2] + [fp32] for k, v in table.items()})
+            timed[fp32] = _class_ms(target, run_mixed, reps)
+        for k in timed[1]:
+            on, off = timed[1][k], timed[0].get(k, timed[1][k])
+            if _key(k) in table:
+                table[_key(k)][2] = 1 if on < 0.99 * off else 0
     apply(target, table)
     return table
 
@@ -66,7 +85,7 @@ def apply(target, table: dict):
     for i, k in enumerate(class_keys()):
         c = table.get(_key(k))
         if c is not None:
-            target.set_tuning(i, int(c[0]), int(c[1]))
+            target.set_tuning(i, int(c[0]), int(c[1]), int(c[2]) if len(c) > 2 else -1)
 
 
 def device_name(device: int) -> str:
@@ -113,7 +132,8 @@ def main():
     dms = torch.as_tensor(clusters.uhf_pair(clusters.atomic_density(mol, 20261204), 20261205),
                           device=dev)
     opt = VHFOpt(mol, 1e-13).build()
-    table = tune(opt, lambda: opt.get_jk(dms, 1), args.reps)
+    table = tune(opt, lambda: opt.get_jk(dms, 1),
+                 lambda: opt.get_jk(dms, 1, mixed_threshold=MIXED_THRESHOLD), args.reps)
     save(dev.index, 'single', table, '(H2O)96 6-31G* UHF pair', args.out)
     print('single', json.dumps(table))
     # batch: uneven 1-24 water clusters, 6-31G*, 1-4 densities
@@ -121,7 +141,8 @@ def main():
     opts = [VHFOpt(m, 1e-13).build() for m, _ in items]
     bd = [torch.as_tensor(d, device=dev) for _, d in items]
     batch = JKBatch(dev.index)
-    table = tune(batch, lambda: batch.build(opts, bd, 1), args.reps)
+    table = tune(batch, lambda: batch.build(opts, bd, 1),
+                 lambda: batch.build(opts, bd, 1, mixed_threshold=MIXED_THRESHOLD), args.reps)
     save(dev.index, 'batch', table, f'{args.batch_mols} water clusters 1-24, 6-31G*', args.out)
     print('batch', json.dumps(table))
 

@@ -145,6 +145,7 @@ class JKBatch:
                    'jk_batch_class_ms')
         return {k: float(ms[i]) for i, k in enumerate(keys) if ms[i] > 0}, launches.value
 
-    def set_tuning(self, cls: int, tasks_per_sm: int, blocks_per_sm: int = 0):
+    def set_tuning(self, cls: int, tasks_per_sm: int, blocks_per_sm: int = 0, fp32: int = -1):
         _lib.check(_lib.lib().jk_batch_set_tuning(self._h, int(cls), int(tasks_per_sm),
-                                                  int(blocks_per_sm)), 'jk_batch_set_tuning')
+                                                  int(blocks_per_sm), int(fp32)),
+                   'jk_batch_set_tuning')

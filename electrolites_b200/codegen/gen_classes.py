@@ -380,8 +380,12 @@ def write_all(outdir, lmax=LMAX):
     reg.append('static const ClassEntry jk_class_table[JK_NCLASSES] = {')
     for A, B, cls in classes:
         form = 0 if cls.form == 'reg' else 1
+        # FP32 quartets by default only in the register-form classes that run
+        # two blocks per SM ((e0|f0) block <= 27); in the larger ones the
+        # second (FP32) copy of the quartet code costs more than it saves
+        fp32 = 1 if cls.form == 'reg' and cls.ne * cls.nf <= 27 else 0
         reg.append(f'    {{{A}, {B}, {cls.li}, {cls.lj}, {cls.lk}, {cls.ll}, '
-                   f'{form}, {1 if cls.form == "reg" else cls.team_threads}, '
+                   f'{form}, {1 if cls.form == "reg" else cls.team_threads}, {fp32}, '
                    f'jk_launch_{cls.tag}}},')
     reg.append('};')
     with open(os.path.join(outdir, 'class_table.inc.tmp'), 'w') as f:

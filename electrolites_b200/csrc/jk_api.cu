@@ -128,6 +128,7 @@ static int rys_tables(int device, const double **rys, const float **rys32)
 struct ClassTune {
     int tasks_per_sm;    // tasks per SM the task size aims at
     int blocks_per_sm;   // cap on resident blocks per SM (0: occupancy limit)
+    int fp32;            // mixed builds may run this class's low-bound quartets in FP32
 };
 
 struct Engine {
@@ -195,6 +196,7 @@ struct jk_plan {
     ShellDev *d_shells = nullptr;
     double *d_basis = nullptr;
     double *d_prim = nullptr;
+    float *d_prim32 = nullptr;      // FP32 copies of the records (mixed form)
     PairRec *d_pairs = nullptr;
     int *d_sh_ao = nullptr, *d_sh_nf = nullptr;
     // ket sub-lists (equal primitive-pair count) per pair class
@@ -227,6 +229,7 @@ static void engine_defaults(Engine &E)
     for (int c = 0; c < JK_NCLASSES; ++c) {
         E.tune[c].tasks_per_sm = jk_class_table[c].form == 0 ? 64 : 16;
         E.tune[c].blocks_per_sm = 0;
+        E.tune[c].fp32 = jk_class_table[c].fp32_default;
     }
 }
 
@@ -468,6 +471,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             v.ket = p->d_pairs + p->pc_off[B];
             v.sub = p->d_subs + p->sub_off[B];
             v.prim = p->d_prim;
+            v.prim32 = p->d_prim32;
             v.dm_cond = it.dmc;
             v.dm_max = it.dm_max;
             v.dmK = it.dm;
@@ -627,7 +631,8 @@ static ClassArgs class_args(const Engine &E, int c, int l, const PlanView **host
     a.row_begin = hv[a.view_begin].row0;
     a.row_end = a.view_begin + a.nvl < a.nviews ? hv[a.view_begin + a.nvl].row0 : a.nrows;
     a.max_bra_prim = E.cls_maxprim[c];
-    a.mixed = E.mixed;
+    a.mixed = E.mixed && E.tune[c].fp32;
+    a.mixed_tab = 0;
     a.shard_rank = E.shard_rank;
     a.shard_size = E.shard_size;
     a.rys = E.rys;
@@ -822,7 +827,7 @@ static int engine_class_ms(Engine &E, float *ms, int ncounts, int *launches)
     return JK_OK;
 }
 
-static int engine_set_tuning(Engine &E, int cls, int tasks_per_sm, int blocks_per_sm)
+static int engine_set_tuning(Engine &E, int cls, int tasks_per_sm, int blocks_per_sm, int fp32)
 {
     if (cls < -1 || cls >= JK_NCLASSES) return fail(JK_ERR_ARG, "tuning: no such class");
     if (tasks_per_sm < 0 || blocks_per_sm < 0) return fail(JK_ERR_ARG, "tuning: negative value");
@@ -832,6 +837,7 @@ static int engine_set_tuning(Engine &E, int cls, int tasks_per_sm, int blocks_pe
         const int def = jk_class_table[cls].form == 0 ? 64 : 16;
         E.tune[cls].tasks_per_sm = tasks_per_sm ? tasks_per_sm : def;
         E.tune[cls].blocks_per_sm = blocks_per_sm;
+        E.tune[cls].fp32 = fp32 < 0 ? jk_class_table[cls].fp32_default : fp32 != 0;
     }
     E.tune_gen++;
     return JK_OK;
@@ -845,6 +851,7 @@ static void free_plan(jk_plan *p)
     cudaFree(p->d_shells);
     cudaFree(p->d_basis);
     cudaFree(p->d_prim);
+    cudaFree(p->d_prim32);
     cudaFree(p->d_pairs);
     cudaFree(p->d_sh_ao);
     cudaFree(p->d_sh_nf);
@@ -972,12 +979,17 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
                            st));
     const size_t prim_bytes = std::max<size_t>(1, rec.size()) * JK_PRIM_STRIDE * sizeof(double);
     CK(cudaMalloc(&p->d_prim, prim_bytes));
-    p->table_bytes += prim_bytes;
+    const size_t prim32_bytes = std::max<size_t>(1, rec.size()) * JK_PRIM32_STRIDE * sizeof(float);
+    CK(cudaMalloc(&p->d_prim32, prim32_bytes));
+    p->table_bytes += prim_bytes + prim32_bytes;
 
     if (!rec.empty()) {
         const int nt = 256;
         prim_pair_fill_kernel<<<(unsigned)((rec.size() + nt - 1) / nt), nt, 0, st>>>(
             tmp.d_rec, (long long)rec.size(), p->d_shells, p->d_basis, p->d_prim);
+        CK(cudaGetLastError());
+        prim32_fill_kernel<<<(unsigned)((rec.size() + nt - 1) / nt), nt, 0, st>>>(
+            p->d_prim, (long long)rec.size(), p->d_prim32);
         CK(cudaGetLastError());
         schwarz_kernel<<<(unsigned)((cand.size() + 127) / 128), 128, 0, st>>>(
             tmp.d_cand, (int)cand.size(), p->d_shells, p->d_prim, p->eng.rys, tmp.d_q);
@@ -1041,8 +1053,8 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
         p->pc_maxprim[k] = mp;
     }
     p->pc_off[NPAIR_CLASSES] = (int)recs.size();
-    for (int k = 0; k < NPAIR_CLASSES; ++k)   // kernels queue ket indices in 29 bits
-        if (p->pc_off[k + 1] - p->pc_off[k] >= (1 << 29))
+    for (int k = 0; k < NPAIR_CLASSES; ++k)   // kernels queue ket indices in 28 bits
+        if (p->pc_off[k + 1] - p->pc_off[k] >= (1 << 28))
             return fail(JK_ERR_ARG, "molecule too large (shell pairs of one class)");
     p->sub_off[NPAIR_CLASSES] = (int)p->subs.size();
     CK(upload(&p->d_subs, p->subs, st, &p->table_bytes));
@@ -1137,10 +1149,11 @@ extern "C" int jk_plan_set_shard(jk_plan *plan, int rank, int size)
     return JK_OK;
 }
 
-extern "C" int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_sm)
+extern "C" int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_sm,
+                                  int fp32)
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_tuning: plan is NULL");
-    return engine_set_tuning(plan->eng, cls, tasks_per_sm, blocks_per_sm);
+    return engine_set_tuning(plan->eng, cls, tasks_per_sm, blocks_per_sm, fp32);
 }
 
 // ---------------------------------------------------------------------------
@@ -1410,10 +1423,11 @@ extern "C" int jk_batch_class_ms(jk_batch *batch, float *ms, int ncounts, int *l
     return engine_class_ms(batch->eng, ms, ncounts, launches);
 }
 
-extern "C" int jk_batch_set_tuning(jk_batch *batch, int cls, int tasks_per_sm, int blocks_per_sm)
+extern "C" int jk_batch_set_tuning(jk_batch *batch, int cls, int tasks_per_sm, int blocks_per_sm,
+                                   int fp32)
 {
     if (!batch) return fail(JK_ERR_ARG, "jk_batch_set_tuning: batch is NULL");
-    return engine_set_tuning(batch->eng, cls, tasks_per_sm, blocks_per_sm);
+    return engine_set_tuning(batch->eng, cls, tasks_per_sm, blocks_per_sm, fp32);
 }
 
 extern "C" int jk_batch_stats(jk_batch *batch, int *graph_replayed, int *graph_captured,

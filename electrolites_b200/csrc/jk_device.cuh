@@ -27,6 +27,9 @@
 #define PR_KP 2     // sqrt(2 pi^5/2) K_ij / a_ij
 #define PR_PX 3     // P (3)
 #define PR_PAX 6    // P - A (3)
+// FP32 copy of the records for the mixed form's single-precision quartets:
+// the same fields as floats, 12 per record (16-byte aligned)
+#define JK_PRIM32_STRIDE 12
 
 struct PairRec {
     int ish, jsh;        // shells; ish carries the higher angular momentum
@@ -45,6 +48,7 @@ struct PlanView {
     const PairRec *ket;      // ket pair class of this plan
     const int2 *sub;         // ket sub-lists [begin, end) within the ket class
     const double *prim;      // prim-pair records of this plan
+    const float *prim32;     // their FP32 copies
     const float *dm_cond;    // nbas x nbas
     const float *dm_max;     // device scalar: max of dm_cond
     // K densities: dmK[0..n_ka) then dmKT[0..n_k-n_ka) (the transposes, for
@@ -73,6 +77,7 @@ struct ClassArgs {
     int view_begin, nvl, row_begin, row_end;
     int max_bra_prim;        // largest primitive-pair count of a bra pair
     int mixed;               // 1: the build has FP32 quartets (mixed form)
+    int mixed_tab;           // 1: the FP32 Rys table is in shared memory (set at launch)
     int shard_rank, shard_size;   // this GPU takes tasks t = rank mod size
     const double *rys;       // Rys table (double): polynomial part + large-x
     const float *rys32;      // Rys table (float)

@@ -23,5 +23,6 @@ struct ClassEntry {
     int li, lj, lk, ll;
     int form;                     // 0 register form, 1 team form
     int team_threads;
+    int fp32_default;             // mixed builds run FP32 quartets here by default
     ClassLauncher launch;
 };

@@ -47,6 +47,19 @@ __global__ void prim_pair_fill_kernel(const int4 *__restrict__ rec, long long nr
     o[9] = 0.;
 }
 
+// FP32 copies of the records (JK_PRIM32_STRIDE floats each) for the mixed
+// form's single-precision quartets
+__global__ void prim32_fill_kernel(const double *__restrict__ prim, long long nrec,
+                                   float *__restrict__ prim32)
+{
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    const double *in = prim + r * JK_PRIM_STRIDE;
+    float *o = prim32 + r * JK_PRIM32_STRIDE;
+#pragma unroll
+    for (int f = 0; f < JK_PRIM32_STRIDE; ++f) o[f] = f < 9 ? (float)in[f] : 0.f;
+}
+
 // ---------------------------------------------------------------------------
 // Schwarz bound per shell pair: q = log sqrt(max_ab |(ab|ab)|), with a
 // runtime-l Rys evaluation (l <= 3).  One thread per pair; O(npairs) work.

@@ -220,11 +220,12 @@ class VHFOpt:
         _lib.check(_lib.lib().jk_plan_set_shard(self.plan, int(rank), int(size)),
                    'jk_plan_set_shard')
 
-    def set_tuning(self, cls: int, tasks_per_sm: int, blocks_per_sm: int = 0):
+    def set_tuning(self, cls: int, tasks_per_sm: int, blocks_per_sm: int = 0, fp32: int = -1):
         """Per-class launch tuning (class index k of class_keys(); -1 resets
         every class)."""
         _lib.check(_lib.lib().jk_plan_set_tuning(self.plan, int(cls), int(tasks_per_sm),
-                                                 int(blocks_per_sm)), 'jk_plan_set_tuning')
+                                                 int(blocks_per_sm), int(fp32)),
+                   'jk_plan_set_tuning')
 
     def memory(self):
         """(bytes of the plan's resident tables, bytes of its build workspace)."""

@@ -176,13 +176,17 @@ int jk_plan_set_shard(jk_plan *plan, int rank, int size);
 
 /*
  * Per-class launch tuning of the plan's builds: the number of tasks per SM
- * the task size aims at, and a cap on resident blocks per SM (0: the
- * occupancy limit).  cls = -1 restores the defaults of every class; a 0
+ * the task size aims at, a cap on resident blocks per SM (0: the occupancy
+ * limit), and whether mixed-precision builds may run this class's
+ * low-bound quartets in FP32 (1 yes, 0 no: FP64 throughout, -1 the class's
+ * default).  cls = -1 restores the defaults of every class; a 0
  * tasks_per_sm restores that class's default.  Set by the autotuner
- * (electrolites_b200/autotune.py); the reference picks its launch shapes in
- * its code generator (electrolites/codegen/gen_khigh.py).
+ * (electrolites_b200/autotune.py), which keeps FP32 only for the classes
+ * where it measures faster; the reference picks its launch shapes in its
+ * code generator (electrolites/codegen/gen_khigh.py).
  */
-int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_sm);
+int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_sm,
+                       int fp32);
 
 /*
  * Batched builds: J/K for many molecules (plans) in one launch stream, each
@@ -222,7 +226,7 @@ int jk_batch_set_timing(jk_batch *batch, int enable);
 int jk_batch_class_ms(jk_batch *batch, float *ms, int ncounts, int *launches);
 /* As jk_plan_set_tuning, for the batch's builds. */
 int jk_batch_set_tuning(jk_batch *batch, int cls, int tasks_per_sm,
-                        int blocks_per_sm);
+                        int blocks_per_sm, int fp32);
 /* Whether the last build replayed or captured a graph, and the batch's
  * device workspace. */
 int jk_batch_stats(jk_batch *batch, int *graph_replayed, int *graph_captured,

@@ -131,12 +131,22 @@ struct ClassTune {
     int fp32;            // mixed builds may run this class's low-bound quartets in FP32
 };
 
+// Class kernels run on this many streams: a persistent class kernel ends
+// with a tail in which the warps that have no task left idle until the last
+// task of the class finishes; on two streams the next class fills those SMs.
+#define JK_CLASS_STREAMS 2
+
 struct Engine {
     int device = 0, num_sms = 148;
-    int *d_rows = nullptr;          // 4 x max_rows: candidates, chunks, chunk prefix, candidate prefix
+    // per class stream: 4 x max_rows ints (candidates, chunks, chunk prefix,
+    // candidate prefix) and CUB scratch of cub_stride bytes
+    int *d_rows = nullptr;
     long long max_rows = 0;
     void *d_cub = nullptr;
-    size_t cub_bytes = 0;
+    size_t cub_bytes = 0, cub_stride = 0;
+    cudaStream_t side[JK_CLASS_STREAMS - 1] = {};   // class streams besides the build's
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[JK_CLASS_STREAMS - 1] = {};
     int *d_chunk = nullptr;         // task size per class
     int *d_counters = nullptr;      // task counter per class launch
     int counter_cap = 0;
@@ -248,6 +258,11 @@ static int engine_init(Engine &E, int device)
     CK(cudaMemset(E.d_error, 0, 2 * sizeof(int)));
     CK(cudaEventCreateWithFlags(&E.blob_ev, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&E.done_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
+    for (int s = 0; s < JK_CLASS_STREAMS - 1; ++s) {
+        CK(cudaStreamCreateWithFlags(&E.side[s], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&E.ev_join[s], cudaEventDisableTiming));
+    }
     return JK_OK;
 }
 
@@ -264,6 +279,11 @@ static void engine_free(Engine &E)
     if (E.h_blob) cudaFreeHost(E.h_blob);
     if (E.blob_ev) cudaEventDestroy(E.blob_ev);
     if (E.done_ev) cudaEventDestroy(E.done_ev);
+    if (E.ev_fork) cudaEventDestroy(E.ev_fork);
+    for (int s = 0; s < JK_CLASS_STREAMS - 1; ++s) {
+        if (E.side[s]) cudaStreamDestroy(E.side[s]);
+        if (E.ev_join[s]) cudaEventDestroy(E.ev_join[s]);
+    }
     for (auto &e : E.ev) cudaEventDestroy(e);
     E = Engine();
 }
@@ -289,12 +309,14 @@ static int engine_reserve_rows(Engine &E, long long rows, bool no_alloc, const c
     E.alloc_gen++;
     size_t cub = 0;
     CK(cub::DeviceScan::InclusiveSum(nullptr, cub, (int *)nullptr, (int *)nullptr, (int)rows));
-    if (cudaMalloc(&E.d_rows, 4 * (size_t)rows * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&E.d_cub, std::max<size_t>(16, cub)) != cudaSuccess) {
+    const size_t stride = align256(std::max<size_t>(16, cub));
+    if (cudaMalloc(&E.d_rows, JK_CLASS_STREAMS * 4 * (size_t)rows * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E.d_cub, JK_CLASS_STREAMS * stride) != cudaSuccess) {
         cudaGetLastError();
         return fail(JK_ERR_NOMEM, std::string(who) + ": cannot allocate the task rows");
     }
     E.cub_bytes = cub;
+    E.cub_stride = stride;
     E.max_rows = rows;
     return JK_OK;
 }
@@ -617,8 +639,11 @@ static int engine_upload(Engine &E, cudaStream_t st)
     return JK_OK;
 }
 
-// launch l of class c: views [l JK_VTAB, ...) of the class
-static ClassArgs class_args(const Engine &E, int c, int l, const PlanView **host_views)
+// the task-row buffers of class stream s
+static int *rows_of(const Engine &E, int s) { return E.d_rows + (size_t)s * 4 * E.max_rows; }
+
+// launch l of class c, on class stream s: views [l JK_VTAB, ...) of the class
+static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView **host_views)
 {
     const PlanView *hv = (const PlanView *)(E.blob.data() + E.off_views) + E.cls_view0[c];
     ClassArgs a;
@@ -639,8 +664,8 @@ static ClassArgs class_args(const Engine &E, int c, int l, const PlanView **host
     a.rys32 = E.rys32;
     a.counter = E.d_counters + E.cls_cnt0[c] + l;
     a.chunk = E.d_chunk + c;
-    a.row_ncand = E.d_rows;
-    a.row_prefix = E.d_rows + 2 * E.max_rows;
+    a.row_ncand = rows_of(E, s);
+    a.row_prefix = rows_of(E, s) + 2 * E.max_rows;
     a.nquartets = E.d_nq + c;
     a.nprimq = E.d_nq + JK_NCLASSES + c;
     a.nquartets32 = E.d_nq + 2 * JK_NCLASSES + c;
@@ -664,7 +689,7 @@ static int engine_configure(Engine &E)
     for (int c = 0; c < JK_NCLASSES; ++c) {
         for (int l = 0; l < E.cls_nlaunch[c]; ++l) {
             const PlanView *hv = nullptr;
-            const ClassArgs a = class_args(E, c, l, &hv);
+            const ClassArgs a = class_args(E, c, l, 0, &hv);
             const int rc = jk_class_table[c].launch(a, hv, cfg);
             if (rc) return fail(JK_ERR_CUDA, std::string("class kernel configuration failed: ") + msg);
         }
@@ -696,38 +721,54 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
     CK(cudaMemsetAsync(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
     char msg[256] = {0};
     LaunchCfg cfg;
-    cfg.stream = st;
     cfg.device = E.device;
     cfg.num_sms = E.num_sms;
     cfg.configure_only = 0;
     cfg.msg = msg;
-    int *chunks = E.d_rows + E.max_rows;
-    int *prefix = E.d_rows + 2 * E.max_rows;
-    int *cand_prefix = E.d_rows + 3 * E.max_rows;
+    // fork the class streams off the build's stream (also inside a capture);
+    // with per-class timing on, one stream, so that each class's events
+    // bracket its own kernels only
+    const int ns = timing ? 1 : JK_CLASS_STREAMS;
+    cudaStream_t cs[JK_CLASS_STREAMS];
+    cs[0] = st;
+    if (ns > 1) CK(cudaEventRecord(E.ev_fork, st));
+    for (int s = 1; s < ns; ++s) {
+        cs[s] = E.side[s - 1];
+        CK(cudaStreamWaitEvent(cs[s], E.ev_fork, 0));
+    }
+    int nactive = 0;
     for (int c = 0; c < JK_NCLASSES; ++c) {
         const int rows = E.cls_rows[c];
         if (!E.cls_nview[c] || rows == 0) continue;
+        const int si = nactive++ % ns;
+        const cudaStream_t cst = cs[si];
+        int *rb = rows_of(E, si);
+        int *chunks = rb + E.max_rows;
+        int *prefix = rb + 2 * E.max_rows;
+        int *cand_prefix = rb + 3 * E.max_rows;
+        void *cub = (char *)E.d_cub + si * E.cub_stride;
         const ClassEntry &ce = jk_class_table[c];
         const PlanView *hv = nullptr;
-        const ClassArgs a = class_args(E, c, 0, &hv);
-        if (timing) CK(cudaEventRecord(E.ev[2 * c], st));
+        const ClassArgs a = class_args(E, c, 0, si, &hv);
+        if (timing) CK(cudaEventRecord(E.ev[2 * c], cst));
         // task list: candidates per row, a task size giving about
         // tasks_per_sm tasks per SM, chunks per row, prefix sum of chunks
-        task_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(a, E.d_rows);
+        task_rows_kernel<<<(rows + 255) / 256, 256, 0, cst>>>(a, rb);
         CK(cudaGetLastError());
         size_t tmp = E.cub_bytes;
-        CK(cub::DeviceScan::InclusiveSum(E.d_cub, tmp, E.d_rows, cand_prefix, rows, st));
+        CK(cub::DeviceScan::InclusiveSum(cub, tmp, rb, cand_prefix, rows, cst));
         const int lo = ce.form == 0 ? 128 : 32, hi = ce.form == 0 ? 4096 : 1024;
         const int target = std::max(1, E.tune[c].tasks_per_sm) * E.num_sms;
-        task_chunks_kernel<<<(rows + 255) / 256, 256, 0, st>>>(E.d_rows, cand_prefix, rows, target,
-                                                               lo, hi, E.d_chunk + c, chunks);
+        task_chunks_kernel<<<(rows + 255) / 256, 256, 0, cst>>>(rb, cand_prefix, rows, target, lo,
+                                                                hi, E.d_chunk + c, chunks);
         CK(cudaGetLastError());
         tmp = E.cub_bytes;
-        CK(cub::DeviceScan::InclusiveSum(E.d_cub, tmp, chunks, prefix, rows, st));
+        CK(cub::DeviceScan::InclusiveSum(cub, tmp, chunks, prefix, rows, cst));
         E.launches += 4;
+        cfg.stream = cst;
         cfg.blocks_per_sm = E.tune[c].blocks_per_sm;
         for (int l = 0; l < E.cls_nlaunch[c]; ++l) {
-            const ClassArgs al = class_args(E, c, l, &hv);
+            const ClassArgs al = class_args(E, c, l, si, &hv);
             int rc;
             {
                 std::lock_guard<std::mutex> lock(g_launch_mutex);
@@ -739,9 +780,14 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
             E.launches++;
         }
         if (timing) {
-            CK(cudaEventRecord(E.ev[2 * c + 1], st));
+            CK(cudaEventRecord(E.ev[2 * c + 1], cst));
             E.ev_used[c] = 1;
         }
+    }
+    // join the class streams back into the build's stream
+    for (int s = 1; s < ns; ++s) {
+        CK(cudaEventRecord(E.ev_join[s - 1], cs[s]));
+        CK(cudaStreamWaitEvent(st, E.ev_join[s - 1], 0));
     }
     if (E.npost) {
         tile_op_kernel<<<(unsigned)E.post_tiles, dim3(32, 8), 0, st>>>(d_post, E.npost);
@@ -1124,8 +1170,10 @@ extern "C" int jk_plan_memory(const jk_plan *plan, long long *table_bytes, long 
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_plan_memory: plan is NULL");
     if (table_bytes)
-        *table_bytes = (long long)(plan->table_bytes + 4 * (size_t)plan->eng.max_rows * sizeof(int) +
-                                   plan->eng.cub_bytes + plan->eng.blob_cap);
+        *table_bytes = (long long)(plan->table_bytes +
+                                   JK_CLASS_STREAMS * (4 * (size_t)plan->eng.max_rows * sizeof(int) +
+                                                       plan->eng.cub_stride) +
+                                   plan->eng.blob_cap);
     if (workspace_bytes) *workspace_bytes = (long long)(plan->eng.ws_size + plan->io_size);
     return JK_OK;
 }
@@ -1438,7 +1486,8 @@ extern "C" int jk_batch_stats(jk_batch *batch, int *graph_replayed, int *graph_c
     if (graph_captured) *graph_captured = batch->last_captured;
     if (workspace_bytes)
         *workspace_bytes = (long long)(batch->eng.ws_size + batch->eng.blob_cap +
-                                       4 * (size_t)batch->eng.max_rows * sizeof(int));
+                                       JK_CLASS_STREAMS * 4 * (size_t)batch->eng.max_rows *
+                                           sizeof(int));
     return JK_OK;
 }
 

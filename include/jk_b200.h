@@ -138,7 +138,9 @@ int jk_class_info(int k, int *li, int *lj, int *lk, int *ll, int *form);
 
 /*
  * Per-class kernel timing.  With enable = 1 every later build records CUDA
- * events around each class kernel on the build's stream;
+ * events around each class kernel and runs all class kernels on the build's
+ * stream (otherwise they are spread over two streams to overlap their
+ * tails);
  * jk_last_class_ms() then returns the milliseconds of each class kernel of
  * the last build (0 for classes not launched) and the number of kernels the
  * library launched in that build.  Synchronises the last build's stream.

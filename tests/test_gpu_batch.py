@@ -206,3 +206,31 @@ def test_mixed_precision_error_and_batch(torch):
         assert _maxdiff(v, mj) <= ATOL
     for v in (bk[0], bk[1]):
         assert _maxdiff(v, mk) <= ATOL
+
+
+def test_split_screening_matches_separate_j_and_k_builds(torch, opts):
+    """J and K terms of a quartet are screened by their own tests, so a J+K
+    build gives the J of a J-only build and the K of a K-only build."""
+    mols, plans = opts
+    o = plans[3]
+    d = torch.as_tensor(dens_stack(mols[3], 2, 1, 13), device='cuda')
+    vj, vk = o.get_jk(d, 1)
+    j_only, _ = o.get_jk(d, 1, with_j=True, with_k=False)
+    _, k_only = o.get_jk(d, 1, with_j=False, with_k=True)
+    assert _maxdiff(vj, j_only) <= 1e-12
+    assert _maxdiff(vk, k_only) <= 1e-12
+
+
+def test_one_or_two_class_streams_agree(torch, opts):
+    """Per-class timing runs every class kernel on one stream; the default
+    spreads them over two.  Both give the same J/K."""
+    mols, plans = opts
+    o = plans[5]
+    d = torch.as_tensor(dens_stack(mols[5], 3, 0, 17), device='cuda')
+    a = o.get_jk(d, 0)
+    o.set_timing(True)
+    b = o.get_jk(d, 0)
+    ms, launches = o.last_class_ms()
+    o.set_timing(False)
+    assert ms and launches > 0
+    assert _maxdiff(a[0], b[0]) <= 1e-12 and _maxdiff(a[1], b[1]) <= 1e-12

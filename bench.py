@@ -309,15 +309,19 @@ def run_serve(args, dev):
     6-31G* or def2-SVP, 1-4 densities, 10 SCF-like cycles with a 1e-4
     relative density perturbation per cycle), continuous batching over
     resident plans with admission by an HBM budget (half the device).
-    Plain and mixed forms at each rate; mols/s and latency percentiles."""
+    Plain and mixed forms at each rate, and the mixed form with incremental
+    builds (cycles between full rebuilds every 5th build J/K of the density
+    change); mols/s and latency percentiles."""
     from electrolites_b200.serve import JKServer, latency_stats, poisson_requests
     out = {'workload': 'serve_h2o3-60_631gs_svp', 'requests': args.serve_requests,
            'cycles': 10, 'hbm_budget': 'half of device memory', 'rates': []}
     for rate in args.serve_rates:
         row = {'rate_req_per_s': rate}
-        for form, thr in (('plain', 0.0), ('mixed', BATCH_MIXED)):
+        for form, thr, inc in (('plain', 0.0, False), ('mixed', BATCH_MIXED, False),
+                               ('mixed_incremental', BATCH_MIXED, True)):
             reqs = poisson_requests(args.serve_requests, rate, SERVE_SEED)
-            srv = JKServer(dev.index, hbm_budget=0.5, mixed_threshold=thr)
+            srv = JKServer(dev.index, hbm_budget=0.5, mixed_threshold=thr, incremental=inc,
+                           rebuild_every=5)
             srv.run(reqs)
             st = latency_stats(reqs)
             row[form] = {k: round(v, 3) for k, v in st.items()}

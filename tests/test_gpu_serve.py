@@ -62,3 +62,23 @@ def test_mixed_serving_energies(torch):
     for p, m in zip(plain, mixed):
         for (pj, pk), (mj, mk) in zip(p.energies, m.energies):
             assert abs(pj - mj) <= 1e-7 and abs(pk - mk) <= 1e-7
+
+
+def test_incremental_serving(torch):
+    """Incremental mode: cycles between full rebuilds build J/K of the
+    density change and add them.  Every cycle's J/K is the same alone and
+    in the mix (1e-10), and within 1e-9 of a full build of that cycle's
+    density (the terms the screening of the change drops are each below
+    direct_scf_tol)."""
+    from electrolites_b200.serve import JKServer, poisson_requests, serve_alone
+    reqs = poisson_requests(4, rate=5000.0, seed=7, n_min=2, n_max=6, cycles=4, keep=True)
+    srv = JKServer(incremental=True, rebuild_every=3)
+    srv.run(reqs)
+    assert max(srv.batch_sizes) > 1
+    for r in reqs:
+        inc_alone = serve_alone(r, incremental=True, rebuild_every=3)
+        full = serve_alone(r)
+        for c, ((mj, mk), (aj, ak), (fj, fk)) in enumerate(zip(r.results, inc_alone, full)):
+            assert np.abs(mj - aj).max() <= ATOL
+            assert np.abs(mk - ak).max() <= ATOL
+            assert np.abs(mj - fj).max() <= 1e-9 and np.abs(mk - fk).max() <= 1e-9

@@ -369,12 +369,16 @@ struct Item {
 struct Spec {
     int hermi, with_j, with_k;
     double mixed_threshold;
+    double omega;                   // > 0: long-range erf(omega r)/r; 0: Coulomb
 };
 
 static int check_spec(const Spec &s, const char *who)
 {
     if (s.hermi < 0 || s.hermi > 2)
         return fail(JK_ERR_ARG, std::string(who) + ": hermi must be 0, 1 or 2");
+    if (!(s.omega >= 0))
+        return fail(JK_ERR_ARG, std::string(who) + ": omega must be >= 0 (short range: "
+                                                    "full minus long range)");
     return JK_OK;
 }
 
@@ -501,6 +505,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             v.dsJ = it.dsJ;
             v.Kh = it.Kh;
             v.Jh = it.Jh;
+            v.inv_om2 = s.omega > 0 ? 1.0 / (s.omega * s.omega) : 0.0;
             v.nbra = nbra;
             v.nket = nket;
             v.nsub = nsub;
@@ -1209,7 +1214,7 @@ extern "C" int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int 
 // ---------------------------------------------------------------------------
 static int build_one(jk_plan *p, const double *dm, int n_dm, int hermi, int with_j, int with_k,
                      double *vj, double *vk, double mixed_threshold, cudaStream_t st, char *ws_ext,
-                     size_t ws_ext_size, bool no_alloc, const char *who)
+                     size_t ws_ext_size, bool no_alloc, const char *who, double omega = 0.0)
 {
     std::vector<Item> items(1);
     items[0].p = p;
@@ -1217,7 +1222,7 @@ static int build_one(jk_plan *p, const double *dm, int n_dm, int hermi, int with
     items[0].n_dm = n_dm;
     items[0].vj = vj;
     items[0].vk = vk;
-    const Spec s{hermi, with_j, with_k, mixed_threshold};
+    const Spec s{hermi, with_j, with_k, mixed_threshold, omega};
     return engine_build(p->eng, items, s, st, ws_ext, ws_ext_size, no_alloc, who);
 }
 
@@ -1228,6 +1233,16 @@ extern "C" int jk_build(jk_plan *plan, const double *dm, int n_dm, int hermi, in
     DeviceGuard g(plan->device);
     return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
                      (cudaStream_t)stream, nullptr, 0, false, "jk_build");
+}
+
+extern "C" int jk_build_rs(jk_plan *plan, const double *dm, int n_dm, int hermi, int with_j,
+                           int with_k, double *vj, double *vk, double mixed_threshold,
+                           double omega, void *stream)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_build_rs: plan is NULL");
+    DeviceGuard g(plan->device);
+    return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
+                     (cudaStream_t)stream, nullptr, 0, false, "jk_build_rs", omega);
 }
 
 extern "C" int jk_sync(jk_plan *plan, void *stream)
@@ -1393,7 +1408,7 @@ extern "C" int jk_batch_build(jk_batch *batch, jk_plan *const *plans, int nplans
         items[i].vj = with_j ? vj[i] : nullptr;
         items[i].vk = with_k ? vk[i] : nullptr;
     }
-    const Spec s{hermi, with_j, with_k, mixed_threshold};
+    const Spec s{hermi, with_j, with_k, mixed_threshold, 0.0};
     batch->last_replayed = batch->last_captured = 0;
     if (!use_graph || !batch->warmed) {
         RC(engine_build(E, items, s, st, nullptr, 0, false, "jk_batch_build"));

@@ -58,6 +58,7 @@ struct PlanView {
     const double *dsJ;
     double *Kh;              // half-K accumulators (n_k, nao, nao)
     double *Jh;              // half-J accumulators (n_j, nao, nao)
+    double inv_om2;          // 1/omega^2 of the long-range operator (0: Coulomb)
     int nbra, nket, nsub, same_class;
     int nbas, nao, n_ka, n_k;
     int n_j;

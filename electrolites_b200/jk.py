@@ -14,8 +14,14 @@ Semantics kept from the reference:
   * vj[k,l] = sum_ij (ij|kl) D[j,i], vk[i,l] = sum_jk (ij|kl) D[j,k];
   * quartets are screened with the direct-SCF threshold of the option
     object: kept when q_ij + q_kl + log max|D| > log(direct_scf_tol);
-  * only the full-range Coulomb operator is served (omega must be 0 or
-    None); anything else raises instead of falling back.
+  * the operator follows PySCF's omega convention: omega = 0 (or None) the
+    Coulomb operator 1/r, omega > 0 the long-range erf(omega r)/r, omega < 0
+    the short-range erfc(|omega| r)/r = 1/r - erf(|omega| r)/r; ``get_k``'s
+    lr_factor / sr_factor ask for lr K_lr + sr K_sr (GPU4PySCF 1.8's
+    range-separated exchange), built as sr K_full + (lr - sr) K_lr.  The
+    reference serves the full and long-range operators and hands the
+    short-range one back (electrolites/fastk.py:642-663,904-925); here all
+    three run on the engine.
 
 The option-object methods work in the Cartesian AO basis of the molecule
 they were built for.  The module functions take densities in the
@@ -119,10 +125,11 @@ class VHFOpt:
         return dms, squeeze
 
     def build_jk_async(self, dms, hermi=1, with_j=True, with_k=True,
-                       vj=None, vk=None, mixed_threshold=0.0, stream=None):
+                       vj=None, vk=None, mixed_threshold=0.0, stream=None, omega=0.0):
         """Enqueue one build on ``stream`` (torch's current stream by default)
         without synchronising; dms must be a contiguous float64 CUDA tensor
-        (n_dm, nao, nao).  Returns (vj, vk)."""
+        (n_dm, nao, nao); omega >= 0 (> 0: the long-range operator).
+        Returns (vj, vk)."""
         torch = _torch()
         plan = self.plan
         n = dms.shape[0]
@@ -132,11 +139,11 @@ class VHFOpt:
             vk = torch.empty_like(dms)
         if stream is None:
             stream = torch.cuda.current_stream(dms.device)
-        _lib.check(_lib.lib().jk_build(
+        _lib.check(_lib.lib().jk_build_rs(
             plan, ctypes.c_void_p(dms.data_ptr()), n, int(hermi), int(bool(with_j)),
             int(bool(with_k)), ctypes.c_void_p(vj.data_ptr() if with_j else 0),
             ctypes.c_void_p(vk.data_ptr() if with_k else 0), float(mixed_threshold),
-            ctypes.c_void_p(stream.cuda_stream)), 'jk_build')
+            float(omega), ctypes.c_void_p(stream.cuda_stream)), 'jk_build_rs')
         return vj, vk
 
     def sync(self, stream=None):
@@ -146,13 +153,27 @@ class VHFOpt:
         _lib.check(_lib.lib().jk_sync(self.plan, ctypes.c_void_p(stream.cuda_stream)),
                    'jk_sync')
 
-    def get_jk(self, dms, hermi=1, verbose=None, with_j=True, with_k=True,
-               mixed_threshold=0.0):
-        """(vj, vk) as CUDA tensors shaped like dms (Cartesian AO basis)."""
-        dms, squeeze = self._prepare(dms)
-        vj, vk = self.build_jk_async(dms, hermi, with_j, with_k,
-                                     mixed_threshold=mixed_threshold)
+    def _combo(self, dms, hermi, with_j, with_k, mixed_threshold, terms):
+        """sum_t c_t (vj, vk)[omega_t] over terms [(c_t, omega_t >= 0)]."""
+        vj = vk = None
+        for c, om in terms:
+            tj, tk = self.build_jk_async(dms, hermi, with_j, with_k,
+                                         mixed_threshold=mixed_threshold, omega=om)
+            if c != 1.0:
+                tj = tj * c if tj is not None else None
+                tk = tk * c if tk is not None else None
+            vj = tj if vj is None else (vj + tj if tj is not None else vj)
+            vk = tk if vk is None else (vk + tk if tk is not None else vk)
         self.sync()
+        return vj, vk
+
+    def get_jk(self, dms, hermi=1, verbose=None, with_j=True, with_k=True,
+               mixed_threshold=0.0, omega=None):
+        """(vj, vk) as CUDA tensors shaped like dms (Cartesian AO basis), for
+        the operator of ``omega`` (PySCF's convention, see the module notes)."""
+        dms, squeeze = self._prepare(dms)
+        vj, vk = self._combo(dms, hermi, with_j, with_k, mixed_threshold,
+                             _rsh_terms(omega, None, None))
         if squeeze:
             vj = vj[0] if vj is not None else None
             vk = vk[0] if vk is not None else None
@@ -160,13 +181,12 @@ class VHFOpt:
 
     def get_k(self, dms, hermi=1, verbose=None, omega=None, lr_factor=None,
               sr_factor=None):
-        _check_omega(omega)
-        _, vk = self.get_jk(dms, hermi, verbose, with_j=False, with_k=True)
-        if lr_factor is not None and sr_factor is not None and lr_factor != sr_factor:
-            raise NotImplementedError('mixed-range exchange is not served')
-        if lr_factor is not None and lr_factor != 1.0:
-            vk = vk * lr_factor
-        return vk
+        """K for lr_factor K_lr + sr_factor K_sr at omega (factors absent: the
+        operator of omega alone)."""
+        dms, squeeze = self._prepare(dms)
+        _, vk = self._combo(dms, hermi, False, True, 0.0,
+                            _rsh_terms(omega, lr_factor, sr_factor))
+        return vk[0] if squeeze else vk
 
     def get_j(self, dms, verbose=None, hermi=1):
         vj, _ = self.get_jk(dms, hermi, verbose, with_j=True, with_k=False)
@@ -257,10 +277,27 @@ def class_keys():
         k += 1
 
 
-def _check_omega(omega):
-    if omega is not None and omega != 0:
-        raise NotImplementedError('only the full-range Coulomb operator is '
-                                  'served (omega = 0)')
+def _rsh_terms(omega, lr_factor, sr_factor):
+    """[(coefficient, omega >= 0), ...] whose combination is the requested
+    operator: lr K_erf(w) + sr K_erfc(w) = sr K_full + (lr - sr) K_erf(w),
+    w = |omega|; without factors omega > 0 is (1, 0) and omega < 0 is (0, 1)."""
+    om = float(omega or 0.0)
+    if lr_factor is None and sr_factor is None:
+        lr, sr = (1.0, 1.0) if om == 0 else ((1.0, 0.0) if om > 0 else (0.0, 1.0))
+    else:
+        lr = 1.0 if lr_factor is None else float(lr_factor)
+        sr = 1.0 if sr_factor is None else float(sr_factor)
+    w = abs(om)
+    if w == 0:
+        if lr != sr:
+            raise ValueError('lr_factor != sr_factor needs omega != 0')
+        return [(lr, 0.0)]
+    terms = []
+    if sr != 0:
+        terms.append((sr, 0.0))
+    if lr - sr != 0:
+        terms.append((lr - sr, w))
+    return terms or [(0.0, 0.0)]
 
 
 # ----------------------------------------------------------------------
@@ -293,7 +330,6 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None,
     """(vj, vk) for densities in mol's AO basis.  numpy in -> numpy out;
     torch in -> torch out."""
     torch = _torch()
-    _check_omega(omega)
     was_numpy = not isinstance(dm, torch.Tensor) and not hasattr(dm, '__cuda_array_interface__')
     opt = _opt_for(mol, vhfopt)
     d = torch.as_tensor(np.asarray(dm) if was_numpy else dm)
@@ -302,7 +338,7 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None,
         d = d[None]
     d = d.to(device=torch.device('cuda', opt.device), dtype=torch.float64)
     dc, c = _to_cart(mol, d)
-    vj, vk = opt.get_jk(dc.contiguous(), hermi, verbose, with_j, with_k)
+    vj, vk = opt.get_jk(dc.contiguous(), hermi, verbose, with_j, with_k, omega=omega)
     outs = []
     for v in (vj, vk):
         if v is None:

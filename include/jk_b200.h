@@ -81,6 +81,19 @@ int jk_build(jk_plan *plan, const double *dm, int n_dm, int hermi,
              double mixed_threshold, void *stream);
 
 /*
+ * jk_build for the long-range operator erf(omega r)/r (omega > 0; omega = 0
+ * is jk_build).  Range-separated exchange (the short-range erfc operator,
+ * lr/sr factor mixtures) is composed from this and jk_build by the caller:
+ * erfc(omega r)/r = 1/r - erf(omega r)/r.  Replaces the reference's
+ * long-range path of _VHFOpt.get_k (electrolites/fastk.py:642-741; the
+ * operator enters its kernels as rsqrt(a_ij + a_kl + a_ij a_kl / omega^2),
+ * electrolites/kernels/fastk_prologue.cu:281-288).
+ */
+int jk_build_rs(jk_plan *plan, const double *dm, int n_dm, int hermi,
+                int with_j, int with_k, double *vj, double *vk,
+                double mixed_threshold, double omega, void *stream);
+
+/*
  * The same with host buffers: copies dm in, builds, copies vj/vk out, and
  * synchronises.  The call a CPU-side caller (PySCF's own get_jk) makes.
  */

@@ -218,9 +218,17 @@ static void cart_comps(int l, int (*c)[3])
 
 #define PRIM_EXP_CUTOFF 60.0   /* drop a primitive pair if exp(-mu R^2) < e^-60 */
 
-/* (ij|kl) for one shell quartet, out[a][b][c][d] in Cartesian components */
+/*
+ * (ij|kl) for one shell quartet, out[a][b][c][d] in Cartesian components.
+ * omega > 0: the long-range operator erf(omega r)/r instead of 1/r.  Its
+ * Rys quadrature is the Coulomb one on the shortened t range
+ * [0, sqrt(theta)], theta = omega^2 / (omega^2 + rho): the roots and weights
+ * at theta x, with the roots (t^2) scaled by theta and the weights by
+ * sqrt(theta) (the reference folds the same change into one fma on
+ * rsqrt(p + q), electrolites/kernels/fastk_prologue.cu:281-288).
+ */
 static void eri_shell_quartet(const Shell *si, const Shell *sj,
-                              const Shell *sk, const Shell *sl, double *out)
+                              const Shell *sk, const Shell *sl, double omega, double *out)
 {
     const int li = si->l, lj = sj->l, lk = sk->l, ll = sl->l;
     const int lij = li + lj, lkl = lk + ll;
@@ -269,11 +277,12 @@ static void eri_shell_quartet(const Shell *si, const Shell *sj,
             }
             const double s = p + q;
             const double rho = p * q / s;
-            const double x = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-            const double fac = PI_FAC / (p * q * sqrt(s)) * kab * kcd;
+            const double theta = omega > 0 ? omega * omega / (omega * omega + rho) : 1.0;
+            const double x = theta * rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+            const double fac = PI_FAC / (p * q * sqrt(s)) * kab * kcd * sqrt(theta);
             oracle_rys(nroots, x, roots, weights);
             for (int r = 0; r < nroots; ++r) {
-                const double u = roots[r];
+                const double u = theta * roots[r];
                 const double b00 = 0.5 * u / s;
                 const double b10 = (1 - q / s * u) / (2 * p);
                 const double b01 = (1 - p / s * u) / (2 * q);
@@ -326,16 +335,22 @@ static void eri_shell_quartet(const Shell *si, const Shell *sj,
     }
 }
 
-int oracle_eri_shells(const int *atm, const int *bas, const double *env,
-                      int ish, int jsh, int ksh, int lsh, double *out)
+int oracle_eri_shells_rs(const int *atm, const int *bas, const double *env,
+                         int ish, int jsh, int ksh, int lsh, double omega, double *out)
 {
     Shell s[4];
     gl_init();
     if (load_shell(&s[0], atm, bas, env, ish) || load_shell(&s[1], atm, bas, env, jsh) ||
         load_shell(&s[2], atm, bas, env, ksh) || load_shell(&s[3], atm, bas, env, lsh))
         return 1;
-    eri_shell_quartet(&s[0], &s[1], &s[2], &s[3], out);
+    eri_shell_quartet(&s[0], &s[1], &s[2], &s[3], omega, out);
     return 0;
+}
+
+int oracle_eri_shells(const int *atm, const int *bas, const double *env,
+                      int ish, int jsh, int ksh, int lsh, double *out)
+{
+    return oracle_eri_shells_rs(atm, bas, env, ish, jsh, ksh, lsh, 0.0, out);
 }
 
 /* q_cond[ish*nbas+jsh] = log(sqrt(max_ab |(ab|ab)|)) for every shell pair */
@@ -351,7 +366,7 @@ int oracle_q_cond(const int *atm, const int *bas, int nbas, const double *env,
         if (load_shell(&si, atm, bas, env, ish)) { err |= 1; continue; }
         for (int jsh = 0; jsh <= ish; ++jsh) {
             if (load_shell(&sj, atm, bas, env, jsh)) { err |= 1; continue; }
-            eri_shell_quartet(&si, &sj, &si, &sj, buf);
+            eri_shell_quartet(&si, &sj, &si, &sj, 0.0, buf);
             int ni = NCART(si.l), nj = NCART(sj.l);
             double m = 0;
             for (int a = 0; a < ni; ++a)
@@ -376,7 +391,8 @@ int oracle_q_cond(const int *atm, const int *bas, int nbas, const double *env,
 static int jk_impl(const int *atm, const int *bas, int nbas, const double *env,
                    const int *ao_loc, const double *dm, int n_dm, double tol,
                    int with_j, int with_k, double *vj, double *vk, int nthreads,
-                   long long *nquartets, const long long *ij_list, long long n_list)
+                   long long *nquartets, const long long *ij_list, long long n_list,
+                   double omega)
 {
     gl_init();
     const int nao = ao_loc[nbas];
@@ -457,7 +473,7 @@ static int jk_impl(const int *atm, const int *bas, int nbas, const double *env,
                     if (q[i * nbas + j] + q[k * nbas + l] + dmax <= log_tol) continue;
                 }
                 count++;
-                eri_shell_quartet(&sh[i], &sh[j], &sh[k], &sh[l], buf);
+                eri_shell_quartet(&sh[i], &sh[j], &sh[k], &sh[l], omega, buf);
                 const int ni = NCART(sh[i].l), nj = NCART(sh[j].l);
                 const int nk = NCART(sh[k].l), nl = NCART(sh[l].l);
                 const int i0 = ao_loc[i], j0 = ao_loc[j], k0 = ao_loc[k], l0 = ao_loc[l];
@@ -524,7 +540,18 @@ int oracle_jk(const int *atm, const int *bas, int nbas, const double *env,
               long long *nquartets)
 {
     return jk_impl(atm, bas, nbas, env, ao_loc, dm, n_dm, tol, with_j, with_k,
-                   vj, vk, nthreads, nquartets, NULL, 0);
+                   vj, vk, nthreads, nquartets, NULL, 0, 0.0);
+}
+
+/* The same for the long-range operator erf(omega r)/r (omega > 0); the
+ * screening keeps the Coulomb Schwarz bounds, an upper bound of it. */
+int oracle_jk_rs(const int *atm, const int *bas, int nbas, const double *env,
+                 const int *ao_loc, const double *dm, int n_dm, double tol,
+                 int with_j, int with_k, double *vj, double *vk, int nthreads,
+                 long long *nquartets, double omega)
+{
+    return jk_impl(atm, bas, nbas, env, ao_loc, dm, n_dm, tol, with_j, with_k,
+                   vj, vk, nthreads, nquartets, NULL, 0, omega);
 }
 
 /*
@@ -538,5 +565,5 @@ int oracle_jk_sample(const int *atm, const int *bas, int nbas, const double *env
                      long long *nquartets, const long long *ij_list, long long n_list)
 {
     return jk_impl(atm, bas, nbas, env, ao_loc, dm, n_dm, tol, with_j, with_k,
-                   vj, vk, nthreads, nquartets, ij_list, n_list);
+                   vj, vk, nthreads, nquartets, ij_list, n_list, 0.0);
 }

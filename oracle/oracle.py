@@ -41,6 +41,9 @@ def lib():
                                 ctypes.POINTER(ctypes.c_longlong)]
         L.oracle_jk_sample.argtypes = L.oracle_jk.argtypes + [
             ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong]
+        L.oracle_eri_shells_rs.argtypes = [ip, ip, dp, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_double, dp]
+        L.oracle_jk_rs.argtypes = L.oracle_jk.argtypes + [ctypes.c_double]
         _lib = L
     return _lib
 
@@ -64,13 +67,14 @@ def rys(n: int, x: float):
     return r, w
 
 
-def eri_shells(mol, i, j, k, l):
+def eri_shells(mol, i, j, k, l, omega=0.0):
+    """(ij|kl) of four shells; omega > 0: the long-range erf(omega r)/r."""
     from electrolites_b200.gto import ncart
     atm, bas, env = _arrays(mol)
     ls = [int(mol._bas[s, 1]) for s in (i, j, k, l)]
     out = np.zeros([ncart(x) for x in ls])
-    if lib().oracle_eri_shells(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
-                               _p(env), i, j, k, l, _p(out)):
+    if lib().oracle_eri_shells_rs(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                                  _p(env), i, j, k, l, float(omega), _p(out)):
         raise ValueError('unsupported shell')
     return out
 
@@ -83,9 +87,9 @@ def q_cond(mol):
     return q
 
 
-def jk(mol, dms, tol=1e-13, with_j=True, with_k=True, nthreads=0):
+def jk(mol, dms, tol=1e-13, with_j=True, with_k=True, nthreads=0, omega=0.0):
     """(vj, vk, n_quartets) for Cartesian-AO densities dms (n_dm, nao, nao);
-    tol <= 0 disables screening."""
+    tol <= 0 disables screening; omega > 0: the long-range erf(omega r)/r."""
     atm, bas, env = _arrays(mol)
     dms = np.ascontiguousarray(dms, dtype=np.float64)
     squeeze = dms.ndim == 2
@@ -95,11 +99,11 @@ def jk(mol, dms, tol=1e-13, with_j=True, with_k=True, nthreads=0):
     vj = np.zeros_like(dms)
     vk = np.zeros_like(dms)
     nq = ctypes.c_longlong(0)
-    err = lib().oracle_jk(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
-                          mol.nbas, _p(env), _p(ao_loc, ctypes.c_int),
-                          _p(dms), dms.shape[0], float(tol), int(with_j),
-                          int(with_k), _p(vj), _p(vk), int(nthreads),
-                          ctypes.byref(nq))
+    err = lib().oracle_jk_rs(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                             mol.nbas, _p(env), _p(ao_loc, ctypes.c_int),
+                             _p(dms), dms.shape[0], float(tol), int(with_j),
+                             int(with_k), _p(vj), _p(vk), int(nthreads),
+                             ctypes.byref(nq), float(omega))
     if err:
         raise RuntimeError(f'oracle_jk failed ({err})')
     if squeeze:

@@ -184,8 +184,9 @@ def test_unsupported_requests_raise(torch):
     from electrolites_b200 import jk
     from electrolites_b200._lib import JKError
     mol = MOLS['h2o_631gs']()
-    with pytest.raises(NotImplementedError):
-        jk.get_k(mol, np.eye(mol.nao), omega=0.3)
+    with pytest.raises(ValueError):   # mixing the ranges needs omega != 0
+        jk.VHFOpt(mol).build().get_k(np.eye(mol.nao_cart), 1, omega=0.0, lr_factor=0.5,
+                                     sr_factor=1.0)
     g = Mole([('H', (0, 0, 0))], basis={'H': [[4, (1.0, 1.0)]]}, cart=True)
     with pytest.raises(JKError, match='unsupported'):
         jk.VHFOpt(g).build()
@@ -206,3 +207,29 @@ def test_host_buffer_entry_point(torch, oracle):
                'jk_build_host')
     rj, rk, _ = oracle.jk(mol, dms, tol=TOL)
     assert np.abs(vj - rj).max() <= ATOL and np.abs(vk - rk).max() <= ATOL
+
+
+@pytest.mark.parametrize('name', ['h2o2_svp', 'spdf'])
+def test_range_separated_operators(torch, oracle, name):
+    """Long-range erf(omega r)/r (omega > 0), short-range erfc (omega < 0)
+    and GPU4PySCF's lr/sr factor mixtures against the oracle (1e-10), on
+    every class up to (ff|ff) for the s/p/d/f molecule."""
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS[name]()
+    rng = np.random.default_rng(21)
+    dms = densities(mol, 'random', 2, 1, rng)
+    opt = VHFOpt(mol, TOL).build()
+    w = 0.4
+    fj, fk, _ = oracle.jk(mol, dms, tol=TOL)
+    lj, lk, _ = oracle.jk(mol, dms, tol=TOL, omega=w)
+    vj, vk = opt.get_jk(torch.as_tensor(dms), 1, omega=w)
+    assert np.abs(vj.cpu().numpy() - lj).max() <= ATOL
+    assert np.abs(vk.cpu().numpy() - lk).max() <= ATOL
+    vj, vk = opt.get_jk(torch.as_tensor(dms), 1, omega=-w)
+    assert np.abs(vj.cpu().numpy() - (fj - lj)).max() <= ATOL
+    assert np.abs(vk.cpu().numpy() - (fk - lk)).max() <= ATOL
+    vk = opt.get_k(torch.as_tensor(dms), 1, omega=w, lr_factor=0.8, sr_factor=0.2)
+    ref = 0.8 * lk + 0.2 * (fk - lk)
+    assert np.abs(vk.cpu().numpy() - ref).max() <= ATOL
+    # the long-range operator is weaker: a smaller K energy in magnitude
+    assert abs(np.einsum('nij,nji->', dms, lk)) < abs(np.einsum('nij,nji->', dms, fk))

@@ -157,3 +157,74 @@ def test_jk_against_explicit_eri_tensor(oracle):
     vj, vk, _ = oracle.jk(mol, D, tol=0)
     np.testing.assert_allclose(vj, np.einsum('ijkl,ji->kl', eri, D), atol=1e-12)
     np.testing.assert_allclose(vk, np.einsum('ijkl,jk->il', eri, D), atol=1e-12)
+
+
+def test_long_range_ssss_closed_form(oracle):
+    """erf(omega r)/r: (ss|ss) = 2 pi^(5/2)/(p q sqrt(p+q)) K K' sqrt(theta)
+    F_0(theta T), theta = omega^2/(omega^2 + rho) (the Boys function of the
+    attenuated operator)."""
+    rng = np.random.default_rng(5)
+    for omega in (0.2, 0.9, 4.0):
+        exps = rng.uniform(0.1, 5, 4)
+        coords = rng.uniform(-1.5, 1.5, (4, 3))
+        mol = four_center_mol(exps, [0, 0, 0, 0], coords)
+        R = mol.atom_coords()
+        a, b, c, d = exps
+        p, q = a + b, c + d
+        P = (a * R[0] + b * R[1]) / p
+        Q = (c * R[2] + d * R[3]) / q
+        kab = math.exp(-a * b / p * np.sum((R[0] - R[1]) ** 2))
+        kcd = math.exp(-c * d / q * np.sum((R[2] - R[3]) ** 2))
+        rho = p * q / (p + q)
+        th = omega ** 2 / (omega ** 2 + rho)
+        T = rho * np.sum((P - Q) ** 2)
+        ref = 2 * math.pi ** 2.5 / (p * q * math.sqrt(p + q)) * kab * kcd * math.sqrt(th) * boys0(th * T)
+        ref *= np.prod([raw_coef(mol, s) for s in range(4)])
+        got = oracle.eri_shells(mol, 0, 1, 2, 3, omega=omega)[0, 0, 0, 0]
+        assert abs(got - ref) <= 1e-14 * abs(ref)
+
+
+@pytest.mark.parametrize('ls', [(1, 1, 1, 1), (3, 2, 2, 1), (3, 3, 3, 3)])
+def test_long_range_limits(oracle, ls):
+    """omega -> infinity gives the Coulomb integrals; the attenuated ones are
+    permutation-symmetric like the Coulomb ones."""
+    rng = np.random.default_rng(sum(ls) + 7)
+    exps = rng.uniform(0.3, 2.0, 4)
+    coords = rng.uniform(-1.2, 1.2, (4, 3))
+    mol = four_center_mol(exps, list(ls), coords)
+    full = oracle.eri_shells(mol, 0, 1, 2, 3)
+    big = oracle.eri_shells(mol, 0, 1, 2, 3, omega=1e7)
+    np.testing.assert_allclose(big, full, rtol=1e-9, atol=1e-12 * np.abs(full).max())
+    lr = oracle.eri_shells(mol, 0, 1, 2, 3, omega=0.5)
+    lr2 = np.transpose(oracle.eri_shells(mol, 2, 3, 0, 1, omega=0.5), (2, 3, 0, 1))
+    np.testing.assert_allclose(lr2, lr, rtol=1e-12, atol=1e-14 * np.abs(lr).max())
+    assert np.abs(lr).max() < np.abs(full).max()
+
+
+def test_long_range_p_from_derivative(oracle):
+    """(p s|s s) of the attenuated operator from the derivative of its s-type
+    integral with respect to the first centre, as for 1/r."""
+    rng = np.random.default_rng(13)
+    exps = np.array([0.9, 1.3, 0.7, 1.1])
+    coords = rng.uniform(-1, 1, (4, 3))
+    bohr = 1 / 0.52917721092
+    h = 1e-3 / bohr
+    a, omega = exps[0], 0.6
+
+    def s_at(dx):
+        c = coords.copy()
+        c[0] += dx
+        mol = four_center_mol(exps, [0, 0, 0, 0], c)
+        v = oracle.eri_shells(mol, 0, 1, 2, 3, omega=omega)[0, 0, 0, 0]
+        return v / np.prod([raw_coef(mol, s) for s in range(4)])
+
+    molp = four_center_mol(exps, [1, 0, 0, 0], coords)
+    vp = oracle.eri_shells(molp, 0, 1, 2, 3, omega=omega)[:, 0, 0, 0]
+    vp /= np.prod([raw_coef(molp, s) for s in range(4)])
+    for d in range(3):
+        e = np.zeros(3)
+        e[d] = h
+        fd1 = (s_at(e) - s_at(-e)) / (2 * h * bohr)
+        fd2 = (s_at(e / 2) - s_at(-e / 2)) / (h * bohr)
+        fd = (4 * fd2 - fd1) / 3
+        assert abs(vp[d] - fd / (2 * a)) <= 1e-8 * max(1e-3, abs(vp[d]))

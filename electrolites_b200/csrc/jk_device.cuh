@@ -17,7 +17,6 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#define JK_PI_FAC 34.986836655249725        // 2 pi^(5/2)
 #define JK_SQRT_PI_FAC 5.914967172795612    // sqrt(2 pi^(5/2))
 
 // primitive-pair record: JK_PRIM_STRIDE doubles, fields at these offsets
@@ -190,9 +189,4 @@ __device__ __forceinline__ void rys_roots(double x, const double *__restrict__ t
         const double v = rys_poly10(c + row * (RYS_DEGREE + 1) / 2, s, s2, s4, s8);
         if (row < N) r[row] = v; else w[row - N] = v;
     }
-}
-
-__device__ __forceinline__ void set_error(int *flag, int code)
-{
-    if (flag) atomicCAS(flag, 0, code);
 }

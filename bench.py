@@ -304,6 +304,35 @@ def run_mixed(args, dev, stream, flush):
     return out
 
 
+RSH_OMEGA, RSH_LR, RSH_SR = 0.3, 1.0, 0.157706   # an omega-B97X-type exchange mixture
+
+
+def run_rsh(args, dev, stream, flush, opt, dms):
+    """Range-separated exchange lr K_erf(w) + sr K_erfc(w) on the main
+    workload (K only, the reference's get_k_rsh): one fused build of
+    sr K_full + (lr - sr) K_lr against the two one-term builds it replaces;
+    device ms per K and the largest element difference."""
+    import torch
+    terms = [(RSH_SR, 0.0), (RSH_LR - RSH_SR, RSH_OMEGA)]
+    vk = torch.empty_like(dms)
+    fused = _timed(lambda: opt.build_jk_async(dms, 1, False, True, None, vk, 0.0, stream,
+                                              terms=terms), 2, 1, stream, flush)
+    opt.sync(stream)
+    ka = torch.empty_like(dms)
+    kb = torch.empty_like(dms)
+
+    def two():
+        opt.build_jk_async(dms, 1, False, True, None, ka, 0.0, stream, terms=terms[:1])
+        opt.build_jk_async(dms, 1, False, True, None, kb, 0.0, stream, terms=terms[1:])
+
+    sep = _timed(two, 2, 1, stream, flush)
+    opt.sync(stream)
+    return {'omega': RSH_OMEGA, 'lr_factor': RSH_LR, 'sr_factor': RSH_SR,
+            'fused_ms': round(fused, 2), 'two_builds_ms': round(sep, 2),
+            'speedup': round(sep / fused, 3),
+            'max_dK': float((vk - ka - kb).abs().max())}
+
+
 def run_serve(args, dev):
     """Serving: Poisson arrivals of water-cluster requests (3-60 waters,
     6-31G* or def2-SVP, 1-4 densities, 10 SCF-like cycles with a 1e-4
@@ -457,6 +486,10 @@ def run_ours(args, rank, world):
     # correctness guard on the timed output: symmetric, finite
     assert torch.isfinite(vj).all() and torch.isfinite(vk).all()
 
+    rsh = None
+    if rank == 0 and world == 1 and not args.no_rsh:
+        rsh = run_rsh(args, dev, stream, flush, opt, dms)
+
     mixed = None
     if rank == 0 and world == 1 and not args.no_mixed:
         mixed = run_mixed(args, dev, stream, flush)
@@ -504,6 +537,7 @@ def run_ours(args, rank, world):
             'clocks': clk,
             'cpu_baseline': cpu,
             'mixed': mixed,
+            'range_separated': rsh,
             'batched': batched,
             'serving': serving,
         }
@@ -526,6 +560,8 @@ def main():
                     help='Poisson arrival rates (requests/s) of the serving runs')
     ap.add_argument('--no-mixed', action='store_true',
                     help='skip the plain-vs-mixed threshold sweep')
+    ap.add_argument('--no-rsh', action='store_true',
+                    help='skip the fused range-separated exchange comparison')
     ap.add_argument('--no-batch', action='store_true',
                     help='skip the uneven-batch comparison (plain vs batched vs mixed)')
     args = ap.parse_args()

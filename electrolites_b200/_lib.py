@@ -19,7 +19,7 @@ JK_ERRORS = {1: 'invalid argument', 2: 'unsupported shell', 3: 'CUDA error',
 EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_build_host', 'jk_sync', 'jk_last_counts', 'jk_class_info',
            'jk_set_timing', 'jk_last_class_ms', 'jk_fp64_peak', 'jk_build_noalloc',
-           'jk_plan_q_cond', 'jk_build_rs', 'jk_plan_memory', 'jk_plan_set_shard',
+           'jk_plan_q_cond', 'jk_build_rs', 'jk_build_op', 'jk_plan_memory', 'jk_plan_set_shard',
            'jk_plan_set_tuning',
            'jk_batch_create', 'jk_batch_destroy', 'jk_batch_build', 'jk_batch_sync',
            'jk_batch_counts', 'jk_batch_set_timing', 'jk_batch_class_ms',
@@ -53,6 +53,8 @@ def lib():
     L.jk_build_host.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, vp]
     L.jk_build_noalloc.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, vp]
     L.jk_build_rs.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, c_double, vp]
+    L.jk_build_op.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, c_int, vp, vp,
+                              vp]
     L.jk_sync.argtypes = [vp, vp]
     L.jk_last_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong),
                                  ctypes.POINTER(ctypes.c_ulonglong),

@@ -167,6 +167,10 @@ struct Engine {
     ClassTune tune[JK_NCLASSES];
     unsigned tune_gen = 0;
     int shard_rank = 0, shard_size = 1;
+    // operator of the prepared build: sum_t op_coef[t] * (1/r, or
+    // erf(omega_t r)/r with op_inv_om2[t] = 1/omega_t^2)
+    int nterm = 1;
+    double op_coef[2] = {1.0, 0.0}, op_inv_om2[2] = {0.0, 0.0};
     bool timing = false;
     std::vector<cudaEvent_t> ev;    // 2 per class
     std::vector<char> ev_used;
@@ -366,19 +370,34 @@ struct Item {
     float *dmc = nullptr, *dm_max = nullptr;
 };
 
+// The operator is sum_t coef[t] * op(omega[t]) over nterm (1 or 2) terms,
+// op(0) = 1/r and op(w > 0) = erf(w r)/r.
 struct Spec {
     int hermi, with_j, with_k;
     double mixed_threshold;
-    double omega;                   // > 0: long-range erf(omega r)/r; 0: Coulomb
+    int nterm;
+    double coef[2];
+    double omega[2];
 };
+
+static Spec coulomb_spec(int hermi, int with_j, int with_k, double mixed_threshold)
+{
+    return Spec{hermi, with_j, with_k, mixed_threshold, 1, {1.0, 0.0}, {0.0, 0.0}};
+}
 
 static int check_spec(const Spec &s, const char *who)
 {
     if (s.hermi < 0 || s.hermi > 2)
         return fail(JK_ERR_ARG, std::string(who) + ": hermi must be 0, 1 or 2");
-    if (!(s.omega >= 0))
-        return fail(JK_ERR_ARG, std::string(who) + ": omega must be >= 0 (short range: "
-                                                    "full minus long range)");
+    if (s.nterm < 1 || s.nterm > 2)
+        return fail(JK_ERR_ARG, std::string(who) + ": the operator takes 1 or 2 terms");
+    for (int t = 0; t < s.nterm; ++t) {
+        if (!(s.omega[t] >= 0) || !std::isfinite(s.omega[t]))
+            return fail(JK_ERR_ARG, std::string(who) + ": omega must be finite and >= 0 (short "
+                                                        "range: full minus long range)");
+        if (!std::isfinite(s.coef[t]))
+            return fail(JK_ERR_ARG, std::string(who) + ": operator coefficients must be finite");
+    }
     return JK_OK;
 }
 
@@ -474,6 +493,12 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     // ---- class views ----
     const float log_mixed = s.mixed_threshold > 0 ? (float)std::log(s.mixed_threshold) : -INFINITY;
     E.mixed = s.mixed_threshold > 0;
+    E.nterm = s.nterm;
+    for (int t = 0; t < 2; ++t) {
+        const bool on = t < s.nterm;
+        E.op_coef[t] = on ? s.coef[t] : 0.0;
+        E.op_inv_om2[t] = on && s.omega[t] > 0 ? 1.0 / (s.omega[t] * s.omega[t]) : 0.0;
+    }
     bool any = false;
     for (const Item &it : items) any = any || it.n_j || it.n_k;
     std::vector<PlanView> views;
@@ -505,7 +530,6 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             v.dsJ = it.dsJ;
             v.Kh = it.Kh;
             v.Jh = it.Jh;
-            v.inv_om2 = s.omega > 0 ? 1.0 / (s.omega * s.omega) : 0.0;
             v.nbra = nbra;
             v.nket = nket;
             v.nsub = nsub;
@@ -665,6 +689,11 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     a.mixed_tab = 0;
     a.shard_rank = E.shard_rank;
     a.shard_size = E.shard_size;
+    a.nterm = E.nterm;
+    for (int t = 0; t < 2; ++t) {
+        a.op_coef[t] = E.op_coef[t];
+        a.op_inv_om2[t] = E.op_inv_om2[t];
+    }
     a.rys = E.rys;
     a.rys32 = E.rys32;
     a.counter = E.d_counters + E.cls_cnt0[c] + l;
@@ -1214,7 +1243,7 @@ extern "C" int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int 
 // ---------------------------------------------------------------------------
 static int build_one(jk_plan *p, const double *dm, int n_dm, int hermi, int with_j, int with_k,
                      double *vj, double *vk, double mixed_threshold, cudaStream_t st, char *ws_ext,
-                     size_t ws_ext_size, bool no_alloc, const char *who, double omega = 0.0)
+                     size_t ws_ext_size, bool no_alloc, const char *who, const Spec *op = nullptr)
 {
     std::vector<Item> items(1);
     items[0].p = p;
@@ -1222,7 +1251,14 @@ static int build_one(jk_plan *p, const double *dm, int n_dm, int hermi, int with
     items[0].n_dm = n_dm;
     items[0].vj = vj;
     items[0].vk = vk;
-    const Spec s{hermi, with_j, with_k, mixed_threshold, omega};
+    Spec s = coulomb_spec(hermi, with_j, with_k, mixed_threshold);
+    if (op) {
+        s.nterm = op->nterm;
+        for (int t = 0; t < 2; ++t) {
+            s.coef[t] = op->coef[t];
+            s.omega[t] = op->omega[t];
+        }
+    }
     return engine_build(p->eng, items, s, st, ws_ext, ws_ext_size, no_alloc, who);
 }
 
@@ -1241,8 +1277,28 @@ extern "C" int jk_build_rs(jk_plan *plan, const double *dm, int n_dm, int hermi,
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_build_rs: plan is NULL");
     DeviceGuard g(plan->device);
+    Spec op = coulomb_spec(hermi, with_j, with_k, mixed_threshold);
+    op.omega[0] = omega;
     return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
-                     (cudaStream_t)stream, nullptr, 0, false, "jk_build_rs", omega);
+                     (cudaStream_t)stream, nullptr, 0, false, "jk_build_rs", &op);
+}
+
+extern "C" int jk_build_op(jk_plan *plan, const double *dm, int n_dm, int hermi, int with_j,
+                           int with_k, double *vj, double *vk, double mixed_threshold,
+                           int n_terms, const double *coef, const double *omega, void *stream)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_build_op: plan is NULL");
+    if (n_terms < 1 || n_terms > 2 || !coef || !omega)
+        return fail(JK_ERR_ARG, "jk_build_op: n_terms must be 1 or 2, with coef and omega");
+    DeviceGuard g(plan->device);
+    Spec op = coulomb_spec(hermi, with_j, with_k, mixed_threshold);
+    op.nterm = n_terms;
+    for (int t = 0; t < n_terms; ++t) {
+        op.coef[t] = coef[t];
+        op.omega[t] = omega[t];
+    }
+    return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
+                     (cudaStream_t)stream, nullptr, 0, false, "jk_build_op", &op);
 }
 
 extern "C" int jk_sync(jk_plan *plan, void *stream)
@@ -1408,7 +1464,7 @@ extern "C" int jk_batch_build(jk_batch *batch, jk_plan *const *plans, int nplans
         items[i].vj = with_j ? vj[i] : nullptr;
         items[i].vk = with_k ? vk[i] : nullptr;
     }
-    const Spec s{hermi, with_j, with_k, mixed_threshold, 0.0};
+    const Spec s = coulomb_spec(hermi, with_j, with_k, mixed_threshold);
     batch->last_replayed = batch->last_captured = 0;
     if (!use_graph || !batch->warmed) {
         RC(engine_build(E, items, s, st, nullptr, 0, false, "jk_batch_build"));

@@ -57,7 +57,6 @@ struct PlanView {
     const double *dsJ;
     double *Kh;              // half-K accumulators (n_k, nao, nao)
     double *Jh;              // half-J accumulators (n_j, nao, nao)
-    double inv_om2;          // 1/omega^2 of the long-range operator (0: Coulomb)
     int nbra, nket, nsub, same_class;
     int nbas, nao, n_ka, n_k;
     int n_j;
@@ -79,6 +78,12 @@ struct ClassArgs {
     int mixed;               // 1: the build has FP32 quartets (mixed form)
     int mixed_tab;           // 1: the FP32 Rys table is in shared memory (set at launch)
     int shard_rank, shard_size;   // this GPU takes tasks t = rank mod size
+    // the operator: sum over nterm (1 or 2) terms of op_coef[t] times the
+    // Coulomb operator (op_inv_om2[t] = 0) or the long-range erf(omega r)/r
+    // (op_inv_om2[t] = 1/omega^2); quartets are screened by the Coulomb bound
+    int nterm;
+    double op_coef[2];
+    double op_inv_om2[2];
     const double *rys;       // Rys table (double): polynomial part + large-x
     const float *rys32;      // Rys table (float)
     int *counter;            // task counter of this launch

@@ -18,7 +18,10 @@ Semantics kept from the reference:
     Coulomb operator 1/r, omega > 0 the long-range erf(omega r)/r, omega < 0
     the short-range erfc(|omega| r)/r = 1/r - erf(|omega| r)/r; ``get_k``'s
     lr_factor / sr_factor ask for lr K_lr + sr K_sr (GPU4PySCF 1.8's
-    range-separated exchange), built as sr K_full + (lr - sr) K_lr.  The
+    range-separated exchange), built as sr K_full + (lr - sr) K_lr in one
+    fused pass (the reference's get_k_rsh, electrolites/fastk.py:774-899:
+    the Rys quadrature runs once per operator inside the primitive loop,
+    screening by the Coulomb bound and the digest are shared).  The
     reference serves the full and long-range operators and hands the
     short-range one back (electrolites/fastk.py:642-663,904-925); here all
     three run on the engine.
@@ -125,25 +128,34 @@ class VHFOpt:
         return dms, squeeze
 
     def build_jk_async(self, dms, hermi=1, with_j=True, with_k=True,
-                       vj=None, vk=None, mixed_threshold=0.0, stream=None, omega=0.0):
+                       vj=None, vk=None, mixed_threshold=0.0, stream=None, omega=0.0,
+                       terms=None):
         """Enqueue one build on ``stream`` (torch's current stream by default)
         without synchronising; dms must be a contiguous float64 CUDA tensor
-        (n_dm, nao, nao); omega >= 0 (> 0: the long-range operator).
-        Returns (vj, vk)."""
+        (n_dm, nao, nao).  The operator is ``terms`` = [(c_t, omega_t >= 0)],
+        one or two of them, sum_t c_t op(omega_t) in one pass (op(0) = 1/r,
+        op(w > 0) = erf(w r)/r); without terms, op(omega).  Returns (vj, vk)."""
         torch = _torch()
         plan = self.plan
         n = dms.shape[0]
+        if terms is None:
+            terms = [(1.0, float(omega))]
+        if not 1 <= len(terms) <= 2:
+            raise ValueError('the operator takes one or two terms')
+        coef = (ctypes.c_double * 2)(*[float(c) for c, _ in terms], *([0.0] * (2 - len(terms))))
+        om = (ctypes.c_double * 2)(*[float(w) for _, w in terms], *([0.0] * (2 - len(terms))))
         if with_j and vj is None:
             vj = torch.empty_like(dms)
         if with_k and vk is None:
             vk = torch.empty_like(dms)
         if stream is None:
             stream = torch.cuda.current_stream(dms.device)
-        _lib.check(_lib.lib().jk_build_rs(
+        _lib.check(_lib.lib().jk_build_op(
             plan, ctypes.c_void_p(dms.data_ptr()), n, int(hermi), int(bool(with_j)),
             int(bool(with_k)), ctypes.c_void_p(vj.data_ptr() if with_j else 0),
             ctypes.c_void_p(vk.data_ptr() if with_k else 0), float(mixed_threshold),
-            float(omega), ctypes.c_void_p(stream.cuda_stream)), 'jk_build_rs')
+            len(terms), ctypes.cast(coef, ctypes.c_void_p), ctypes.cast(om, ctypes.c_void_p),
+            ctypes.c_void_p(stream.cuda_stream)), 'jk_build_op')
         return vj, vk
 
     def sync(self, stream=None):
@@ -154,16 +166,10 @@ class VHFOpt:
                    'jk_sync')
 
     def _combo(self, dms, hermi, with_j, with_k, mixed_threshold, terms):
-        """sum_t c_t (vj, vk)[omega_t] over terms [(c_t, omega_t >= 0)]."""
-        vj = vk = None
-        for c, om in terms:
-            tj, tk = self.build_jk_async(dms, hermi, with_j, with_k,
-                                         mixed_threshold=mixed_threshold, omega=om)
-            if c != 1.0:
-                tj = tj * c if tj is not None else None
-                tk = tk * c if tk is not None else None
-            vj = tj if vj is None else (vj + tj if tj is not None else vj)
-            vk = tk if vk is None else (vk + tk if tk is not None else vk)
+        """(vj, vk) of the operator sum_t c_t op(omega_t) over terms
+        [(c_t, omega_t >= 0)], one fused build."""
+        vj, vk = self.build_jk_async(dms, hermi, with_j, with_k,
+                                     mixed_threshold=mixed_threshold, terms=terms)
         self.sync()
         return vj, vk
 

@@ -82,16 +82,33 @@ int jk_build(jk_plan *plan, const double *dm, int n_dm, int hermi,
 
 /*
  * jk_build for the long-range operator erf(omega r)/r (omega > 0; omega = 0
- * is jk_build).  Range-separated exchange (the short-range erfc operator,
- * lr/sr factor mixtures) is composed from this and jk_build by the caller:
- * erfc(omega r)/r = 1/r - erf(omega r)/r.  Replaces the reference's
- * long-range path of _VHFOpt.get_k (electrolites/fastk.py:642-741; the
- * operator enters its kernels as rsqrt(a_ij + a_kl + a_ij a_kl / omega^2),
+ * is jk_build).  Replaces the reference's long-range path of
+ * _VHFOpt.get_k (electrolites/fastk.py:642-741; the operator enters its
+ * kernels as rsqrt(a_ij + a_kl + a_ij a_kl / omega^2),
  * electrolites/kernels/fastk_prologue.cu:281-288).
  */
 int jk_build_rs(jk_plan *plan, const double *dm, int n_dm, int hermi,
                 int with_j, int with_k, double *vj, double *vk,
                 double mixed_threshold, double omega, void *stream);
+
+/*
+ * jk_build for the operator sum_t coef[t] * op(omega[t]) over n_terms (1 or
+ * 2) terms, op(0) = 1/r and op(w > 0) = erf(w r)/r, in one pass over the
+ * shell quartets: each primitive quartet evaluates the Rys quadrature once
+ * per term, and screening, primitive data and the density contraction are
+ * shared.  Range-separated exchange lr K_erf + sr K_erfc is
+ * {sr, lr - sr} at {0, omega} (erfc(w r)/r = 1/r - erf(w r)/r).
+ * Quartets are screened by their Coulomb bound, without the coefficients.
+ * Replaces the reference's fused two-range K, get_k_rsh
+ * (electrolites/fastk.py:774-899: coef_f K_full + coef_l K_lr in a single
+ * pass, screened with the full-range q_cond); here J takes the same operator
+ * when with_j is set.  Errors: n_terms outside 1..2, a negative or
+ * non-finite omega, a non-finite coefficient.
+ */
+int jk_build_op(jk_plan *plan, const double *dm, int n_dm, int hermi,
+                int with_j, int with_k, double *vj, double *vk,
+                double mixed_threshold, int n_terms, const double *coef,
+                const double *omega, void *stream);
 
 /*
  * The same with host buffers: copies dm in, builds, copies vj/vk out, and

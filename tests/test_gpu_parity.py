@@ -233,3 +233,105 @@ def test_range_separated_operators(torch, oracle, name):
     assert np.abs(vk.cpu().numpy() - ref).max() <= ATOL
     # the long-range operator is weaker: a smaller K energy in magnitude
     assert abs(np.einsum('nij,nji->', dms, lk)) < abs(np.einsum('nij,nji->', dms, fk))
+
+
+@pytest.mark.parametrize('name', ['h2o2_svp', 'spdf'])
+def test_fused_two_term_operator(torch, oracle, name):
+    """One fused build of c0 op(0) + c1 op(w) (both terms inside the
+    primitive loop, one screening and digest) equals the sum of the two
+    one-term builds (1e-12) and the oracle's (1e-10), for J and K of a
+    general (hermi 0) density; FP32 quartets of the mixed form keep the
+    energies within 1e-7 Eh."""
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS[name]()
+    dms = densities(mol, 'random', 2, 0, np.random.default_rng(23))
+    opt = VHFOpt(mol, TOL).build()
+    d = torch.as_tensor(dms, device='cuda')
+    c0, c1, w = 0.35, -1.25, 0.3
+    fj, fk = opt.build_jk_async(d, 0, terms=[(c0, 0.0), (c1, w)])
+    aj, ak = opt.build_jk_async(d, 0, terms=[(c0, 0.0)])
+    bj, bk = opt.build_jk_async(d, 0, terms=[(c1, w)])
+    opt.sync()
+    assert float((fj - aj - bj).abs().max()) <= 1e-12
+    assert float((fk - ak - bk).abs().max()) <= 1e-12
+    rj, rk, _ = oracle.jk(mol, dms, tol=TOL)
+    lj, lk, _ = oracle.jk(mol, dms, tol=TOL, omega=w)
+    assert np.abs(fj.cpu().numpy() - (c0 * rj + c1 * lj)).max() <= ATOL
+    assert np.abs(fk.cpu().numpy() - (c0 * rk + c1 * lk)).max() <= ATOL
+    mj, mk = opt.build_jk_async(d, 0, mixed_threshold=1e-6, terms=[(c0, 0.0), (c1, w)])
+    opt.sync()
+    ej, ek = _energies(dms, fj.cpu().numpy(), fk.cpu().numpy())
+    mej, mek = _energies(dms, mj.cpu().numpy(), mk.cpu().numpy())
+    assert abs(ej - mej) <= 1e-7 and abs(ek - mek) <= 1e-7
+
+
+def test_operator_arguments_rejected(torch):
+    from electrolites_b200 import _lib
+    from electrolites_b200.jk import VHFOpt
+    mol = MOLS['h2o2_svp']()
+    opt = VHFOpt(mol, TOL).build()
+    d = torch.zeros((1, mol.nao_cart, mol.nao_cart), dtype=torch.float64, device='cuda')
+    with pytest.raises(ValueError):
+        opt.build_jk_async(d, 1, terms=[(1.0, 0.0), (1.0, 0.2), (1.0, 0.3)])
+    with pytest.raises(_lib.JKError, match='omega'):
+        opt.build_jk_async(d, 1, terms=[(1.0, 0.0), (1.0, -0.2)])
+    with pytest.raises(_lib.JKError, match='coefficients'):
+        opt.build_jk_async(d, 1, terms=[(float('nan'), 0.0)])
+    vj, vk = opt.get_jk(d, 1)
+    assert float(vk.abs().max()) == 0.0
+
+
+class _GeneralContraction:
+    """A molecule in PySCF's layout whose shells carry several contractions
+    (nctr > 1): built from a molecule with one contraction per shell by
+    merging runs of shells on one atom with the same l and exponents.  The
+    AO order (contraction-major inside a shell) equals the split one."""
+
+    def __init__(self, split):
+        bas, env = [], list(split._env)
+        rows = [list(r) for r in split._bas]
+        s = 0
+        while s < len(rows):
+            ia, l, nprim, _, _, pe, pc, _ = rows[s]
+            e = s + 1
+            while (e < len(rows) and rows[e][0] == ia and rows[e][1] == l
+                   and rows[e][2] == nprim
+                   and list(split._env[rows[e][5]:rows[e][5] + nprim]) ==
+                   list(split._env[pe:pe + nprim])):
+                e += 1
+            pc_new = len(env)
+            for t in range(s, e):
+                env.extend(split._env[rows[t][6]:rows[t][6] + nprim])
+            bas.append([ia, l, nprim, e - s, 0, pe, pc_new, 0])
+            s = e
+        self._atm = split._atm
+        self._bas = np.asarray(bas, dtype=np.int32)
+        self._env = np.asarray(env)
+        self.nbas = len(bas)
+        self.cart = True
+
+    def ao_loc_nr(self, cart=True):
+        n = [(l + 1) * (l + 2) // 2 * nctr for l, nctr in zip(self._bas[:, 1], self._bas[:, 3])]
+        return np.concatenate([[0], np.cumsum(n)]).astype(np.int32)
+
+
+def test_general_contractions(torch, oracle):
+    """Shells with several contractions are expanded contraction-major, as
+    PySCF orders their AOs: J/K equal the oracle on the split molecule."""
+    from electrolites_b200.jk import VHFOpt
+    b = {'C': [[1, (1.2, 0.5), (0.4, 0.4), (0.1, 0.2)],
+               [1, (1.2, -0.3), (0.4, 0.2), (0.1, 0.7)],
+               [0, (3.0, 0.6), (0.7, 0.5)],
+               [0, (3.0, 0.1), (0.7, -0.9)],
+               [2, (0.8, 1.0)]],
+         'H': [[0, (1.3, 0.6), (0.3, 0.5)], [1, (0.9, 1.0)]]}
+    split = Mole([('C', (0.0, 0.0, 0.0)), ('H', (0.7, 0.5, -0.4)), ('H', (-0.8, 0.3, 0.6))],
+                 basis=b, cart=True)
+    gc = _GeneralContraction(split)
+    assert gc.nbas < split.nbas and int(gc._bas[:, 3].max()) == 2
+    rng = np.random.default_rng(31)
+    dms = densities(split, 'random', 2, 0, rng)
+    rj, rk, _ = oracle.jk(split, dms, tol=TOL)
+    vj, vk = VHFOpt(gc, TOL).build().get_jk(torch.as_tensor(dms), 0)
+    assert np.abs(vj.cpu().numpy() - rj).max() <= ATOL
+    assert np.abs(vk.cpu().numpy() - rk).max() <= ATOL

@@ -333,6 +333,63 @@ def run_rsh(args, dev, stream, flush, opt, dms):
             'max_dK': float((vk - ka - kb).abs().max())}
 
 
+SCF_CYCLES, SCF_SIGMA0, SCF_DECAY, SCF_SEED = 14, 3e-2, 0.5, 20261207
+
+
+def run_scf_screen(args, dev, stream, opt, dms_h):
+    """Loose-then-tight screening (the reference's fastscfscreen) on a
+    synthetic SCF-like trajectory of the main workload: cycle c moves the
+    densities by symmetric noise of SCF_SIGMA0 * SCF_DECAY**c * max|D|.
+    Tight incremental builds (J/K of D - D_last at direct_scf_tol from the
+    second cycle on) against the loose-then-tight schedule (step: the AO
+    density change); device ms summed over the cycles, the schedule's
+    decisions, and each final J/K against a full tight build of the final
+    density."""
+    import torch
+
+    from electrolites_b200 import screen
+    from electrolites_b200.serve import advance_density
+
+    def trajectory(loose_tight):
+        d = torch.as_tensor(dms_h, device=dev).contiguous()
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SCF_SEED)
+        lt = screen.LooseTightJK(opt) if loose_tight else None
+        vj = vk = last = None
+        total = 0.0
+        with torch.cuda.stream(stream):
+            for c in range(SCF_CYCLES):
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                if lt is not None:
+                    vj, vk = lt.jk(d)
+                elif last is None:
+                    vj, vk = opt.get_jk(d, 1)
+                else:
+                    dj, dk = opt.get_jk(d - last, 1)
+                    vj, vk = vj + dj, vk + dk
+                e.record(stream)
+                e.synchronize()
+                total += s.elapsed_time(e)
+                last = d.clone()
+                if c + 1 < SCF_CYCLES:
+                    advance_density(d, SCF_SIGMA0 * SCF_DECAY ** c, gen)
+            fj, fk = opt.get_jk(d, 1)
+        out = {'ms': round(total, 2), 'final_max_dJ': float((vj - fj).abs().max()),
+               'final_max_dK': float((vk - fk).abs().max())}
+        if lt is not None:
+            out['decisions'] = {k: lt.decisions.count(k) for k in
+                                (screen.FULL, screen.LOOSE_INC, screen.REBUILD, screen.TIGHT_INC)}
+        return out
+
+    tight = trajectory(False)
+    lt = trajectory(True)
+    return {'cycles': SCF_CYCLES, 'sigma0': SCF_SIGMA0, 'decay': SCF_DECAY,
+            'loose': screen.LOOSE, 'switch': screen.SWITCH, 'step': 'AO density change',
+            'tight_incremental': tight, 'loose_then_tight': lt,
+            'speedup': round(tight['ms'] / lt['ms'], 3)}
+
+
 def run_serve(args, dev):
     """Serving: Poisson arrivals of water-cluster requests (3-60 waters,
     6-31G* or def2-SVP, 1-4 densities, 10 SCF-like cycles with a 1e-4
@@ -490,6 +547,10 @@ def run_ours(args, rank, world):
     if rank == 0 and world == 1 and not args.no_rsh:
         rsh = run_rsh(args, dev, stream, flush, opt, dms)
 
+    scf_screen = None
+    if rank == 0 and world == 1 and not args.no_scf_screen:
+        scf_screen = run_scf_screen(args, dev, stream, opt, dms_h)
+
     mixed = None
     if rank == 0 and world == 1 and not args.no_mixed:
         mixed = run_mixed(args, dev, stream, flush)
@@ -538,6 +599,7 @@ def run_ours(args, rank, world):
             'cpu_baseline': cpu,
             'mixed': mixed,
             'range_separated': rsh,
+            'loose_then_tight': scf_screen,
             'batched': batched,
             'serving': serving,
         }
@@ -560,6 +622,8 @@ def main():
                     help='Poisson arrival rates (requests/s) of the serving runs')
     ap.add_argument('--no-mixed', action='store_true',
                     help='skip the plain-vs-mixed threshold sweep')
+    ap.add_argument('--no-scf-screen', action='store_true',
+                    help='skip the loose-then-tight screening trajectory')
     ap.add_argument('--no-rsh', action='store_true',
                     help='skip the fused range-separated exchange comparison')
     ap.add_argument('--no-batch', action='store_true',

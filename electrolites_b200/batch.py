@@ -81,7 +81,7 @@ class JKBatch:
             vj = [torch.empty_like(d) for d in dms]
         if with_k and vk is None:
             vk = [torch.empty_like(d) for d in dms]
-        plans = (ctypes.c_void_p * n)(*[o.plan.value for o in opts])
+        plans = (ctypes.c_void_p * n)(*[o.apply_tol().value for o in opts])
         dmp = (ctypes.c_void_p * n)(*[d.data_ptr() for d in dms])
         ndm = (ctypes.c_int * n)(*[d.shape[0] for d in dms])
         vjp = (ctypes.c_void_p * n)(*[v.data_ptr() for v in vj]) if with_j else None

@@ -199,6 +199,10 @@ struct jk_plan {
     std::vector<int> sh_l, sh_ao, sh_user;
     double tol = 1e-13;
     float log_tol = 0.f;
+    // screening threshold of the builds: the plan's own or a looser one
+    // (jk_plan_set_tol), never tighter than the pair lists were made for
+    double build_tol = 1e-13;
+    float build_log_tol = 0.f;
     float q_max = -INFINITY, q_drop_max = -INFINITY;
     long long npairs = 0;
     long long max_rows = 0;         // largest bra-class pairs x ket-class sub-lists
@@ -539,7 +543,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             v.n_ka = it.n_ka;
             v.n_k = it.n_k;
             v.n_j = it.n_j;
-            v.log_tol = p->log_tol;
+            v.log_tol = p->build_log_tol;
             v.mixed_log_thr = log_mixed;
             v.row0 = (int)rows;
             rows += (long long)nbra * nsub;
@@ -623,7 +627,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         ci.blk0 = cblk;
         ci.q_drop = it.p->q_drop_max;
         ci.q_max = it.p->q_max;
-        ci.log_tol = it.p->log_tol;
+        ci.log_tol = it.p->build_log_tol;
         ci.pad = 0;
         cblk += (long long)ci.nt * ci.nt;
         cond.push_back(ci);
@@ -979,6 +983,8 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     p->device = device;
     p->tol = tol;
     p->log_tol = (float)std::log(tol);
+    p->build_tol = tol;
+    p->build_log_tol = p->log_tol;
     p->nbas_user = nbas_user;
     RC(engine_init(p->eng, device));
 
@@ -1228,6 +1234,23 @@ extern "C" int jk_plan_set_shard(jk_plan *plan, int rank, int size)
         return fail(JK_ERR_ARG, "jk_plan_set_shard: need 0 <= rank < size");
     plan->eng.shard_rank = rank;
     plan->eng.shard_size = size;
+    return JK_OK;
+}
+
+extern "C" int jk_plan_set_tol(jk_plan *plan, double tol)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_tol: plan is NULL");
+    if (!(tol > 0) || !std::isfinite(tol))
+        return fail(JK_ERR_ARG, "jk_plan_set_tol: tol must be positive and finite");
+    if (tol < plan->tol) {
+        char msg[200];
+        snprintf(msg, sizeof(msg),
+                 "jk_plan_set_tol: tol %g is below the plan's threshold %g (its pair lists "
+                 "would miss quartets): create a new plan", tol, plan->tol);
+        return fail(JK_ERR_ARG, msg);
+    }
+    plan->build_tol = tol;
+    plan->build_log_tol = tol == plan->tol ? plan->log_tol : (float)std::log(tol);
     return JK_OK;
 }
 

@@ -90,6 +90,7 @@ class VHFOpt:
                    'jk_plan_info')
         self.nao = nao.value
         self.npairs = npairs.value
+        self._plan_tol = self._applied_tol = self.direct_scf_tol
         from . import autotune
         table = autotune.load(self.device, 'single')
         if table:
@@ -109,6 +110,18 @@ class VHFOpt:
         if self._plan is None:
             self.build()
         return self._plan
+
+    def apply_tol(self):
+        """Hands ``direct_scf_tol`` to the plan if it changed since the last
+        build: builds read it at call time, as the reference's do.  A value
+        below the threshold the plan was built with is an error (its pair
+        lists lack the pairs a tighter screen needs)."""
+        plan = self.plan
+        tol = float(self.direct_scf_tol)
+        if tol != self._applied_tol:
+            _lib.check(_lib.lib().jk_plan_set_tol(plan, tol), 'jk_plan_set_tol')
+            self._applied_tol = tol
+        return plan
 
     # ------------------------------------------------------------------
     def _prepare(self, dms):
@@ -136,7 +149,7 @@ class VHFOpt:
         one or two of them, sum_t c_t op(omega_t) in one pass (op(0) = 1/r,
         op(w > 0) = erf(w r)/r); without terms, op(omega).  Returns (vj, vk)."""
         torch = _torch()
-        plan = self.plan
+        plan = self.apply_tol()
         n = dms.shape[0]
         if terms is None:
             terms = [(1.0, float(omega))]

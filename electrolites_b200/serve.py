@@ -24,7 +24,14 @@ cycle together in one batched build (electrolites_b200.batch.JKBatch):
     adds them to the previous J/K; the change is small (1e-4 of D per cycle
     here), so the density-weighted screening drops most quartets.  Every
     `rebuild_every`-th cycle is a full build, which bounds the drift from
-    terms the screening dropped.
+    terms the screening dropped;
+  * loose-then-tight screening (optional, with incremental mode): each
+    request follows the schedule of electrolites_b200.screen.ScreenPhase
+    (the reference's electrolites/fastscfscreen.py) in place of the
+    periodic rebuilds: incremental builds at a loose threshold while its
+    density step is large, one tight rebuild at the switch, tight increments
+    after it.  Requests in different phases share one batched build (each
+    plan screens at its own threshold).
 
 Latency of a request = completion of its last cycle - its arrival.  The
 reference has no serving layer; this sits on top of the same J/K call the
@@ -38,6 +45,7 @@ import time
 
 import numpy as np
 
+from . import screen
 from .batch import JKBatch
 from .jk import VHFOpt
 
@@ -54,6 +62,7 @@ class Request:
     dms: np.ndarray                # (n_dm, nao, nao) Cartesian, first cycle
     cycles: int = 10
     sigma: float = 1e-4            # per-cycle symmetric perturbation, relative to max|D|
+    sigma_decay: float = 1.0       # the perturbation of cycle c is sigma * sigma_decay**c
     arrival: float = 0.0           # seconds after the start of the run
     seed: int = 0
     keep: bool = False             # keep every cycle's (vj, vk) on the host
@@ -90,7 +99,7 @@ def advance_density(d, sigma, gen):
 
 class _Active:
     __slots__ = ('req', 'opt', 'dms', 'vj', 'vk', 'gen', 'bytes', 'prev', 'delta', 'jacc', 'kacc',
-                 'inc')
+                 'inc', 'screen')
 
     def j(self):
         return self.jacc if self.jacc is not None else self.vj
@@ -104,7 +113,9 @@ class JKServer:
 
     def __init__(self, device: int | None = None, hbm_budget: float = 0.5,
                  max_active: int = 512, mixed_threshold: float = 0.0, tol: float = 1e-13,
-                 use_graph: bool = False, incremental: bool = False, rebuild_every: int = 5):
+                 use_graph: bool = False, incremental: bool = False, rebuild_every: int = 5,
+                 loose_tight: bool = False, loose: float = screen.LOOSE,
+                 switch: float = screen.SWITCH, max_loose: int = screen.MAX_LOOSE):
         torch = _torch()
         self.device = torch.cuda.current_device() if device is None else int(device)
         self.dev = torch.device('cuda', self.device)
@@ -117,6 +128,10 @@ class JKServer:
         self.use_graph = use_graph
         self.incremental = incremental
         self.rebuild_every = max(1, int(rebuild_every))
+        if loose_tight and not incremental:
+            raise ValueError('loose-then-tight screening needs incremental mode')
+        self.loose_tight = loose_tight
+        self.screen_args = (loose, switch, max_loose)
         self.batch = JKBatch(self.device)
         self.stream = torch.cuda.Stream(self.dev)         # batched builds, density updates
         self.admit_stream = torch.cuda.Stream(self.dev)   # uploads of admitted requests
@@ -125,6 +140,7 @@ class JKServer:
         self.used = 0
         self.iterations = 0
         self.batch_sizes = []
+        self.screen_stats = {'loose_builds': 0, 'rebuilds': 0, 'tight_builds': 0, 'capped': 0}
 
     # ------------------------------------------------------------------
     def _admit(self, now):
@@ -156,6 +172,7 @@ class JKServer:
                     a.jacc = torch.empty_like(a.dms)
                     a.kacc = torch.empty_like(a.dms)
             a.inc = False
+            a.screen = screen.ScreenPhase(*self.screen_args) if self.loose_tight else None
             a.gen = torch.Generator(device=self.dev)
             a.gen.manual_seed(req.seed)
             tables, _ = a.opt.memory()
@@ -171,7 +188,13 @@ class JKServer:
         out = []
         with torch.cuda.stream(self.stream):
             for a in self.active:
-                a.inc = self.incremental and a.req.done_cycles % self.rebuild_every != 0
+                if a.screen is not None:
+                    d = a.screen.decide(a.req.done_cycles > 0,
+                                        lambda: screen.density_step(a.dms, a.prev))
+                    a.inc = d in (screen.LOOSE_INC, screen.TIGHT_INC)
+                    a.opt.direct_scf_tol = a.screen.tol(d, self.tol)
+                else:
+                    a.inc = self.incremental and a.req.done_cycles % self.rebuild_every != 0
                 if a.inc:
                     torch.sub(a.dms, a.prev, out=a.delta)
                     out.append(a.delta)
@@ -203,9 +226,12 @@ class JKServer:
             if req.done_cycles >= req.cycles:
                 req.finished = now
                 self.used -= a.bytes
+                if a.screen is not None:
+                    for key, v in a.screen.stats.items():
+                        self.screen_stats[key] += v
                 continue
             with torch.cuda.stream(self.stream):
-                advance_density(a.dms, req.sigma, a.gen)
+                advance_density(a.dms, req.sigma * req.sigma_decay ** (req.done_cycles - 1), a.gen)
             still.append(a)
         self.active = still
 
@@ -256,7 +282,7 @@ def latency_stats(requests):
 
 def poisson_requests(n: int, rate: float, seed: int, n_min: int = 3, n_max: int = 60,
                      bases=('6-31g*', 'def2-svp'), cycles: int = 10, sigma: float = 1e-4,
-                     keep: bool = False):
+                     keep: bool = False, sigma_decay: float = 1.0):
     """n requests with exponential inter-arrival times (rate per second):
     water clusters of n_min..n_max waters (cube edge 3.1 n^(1/3) A), a basis
     drawn from `bases`, 1-4 densities."""
@@ -273,25 +299,31 @@ def poisson_requests(n: int, rate: float, seed: int, n_min: int = 3, n_max: int 
         mol = clusters.water_mole(nw, 3.1 * nw ** (1.0 / 3.0), s, basis=basis)
         dms = clusters.density_stack(clusters.atomic_density(mol, s), k, s + 1)
         out.append(Request(rid=i, mol=mol, dms=dms, cycles=cycles, sigma=sigma, arrival=t,
-                           seed=s, keep=keep))
+                           seed=s, keep=keep, sigma_decay=sigma_decay))
     return out
 
 
 def serve_alone(req: Request, device: int | None = None, mixed_threshold: float = 0.0,
-                tol: float = 1e-13, incremental: bool = False, rebuild_every: int = 5):
+                tol: float = 1e-13, incremental: bool = False, rebuild_every: int = 5,
+                loose_tight: bool = False, loose: float = screen.LOOSE,
+                switch: float = screen.SWITCH, max_loose: int = screen.MAX_LOOSE):
     """The same request served by itself: one build per cycle on its own
-    plan, the same density updates (and the same incremental schedule).
-    Returns [(vj, vk), ...] per cycle."""
+    plan, the same density updates (and the same incremental or
+    loose-then-tight schedule).  Returns [(vj, vk), ...] per cycle."""
     torch = _torch()
     dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
     opt = VHFOpt(req.mol, tol, device=dev.index).build()
     d = torch.as_tensor(req.dms, device=dev).contiguous()
     gen = torch.Generator(device=dev)
     gen.manual_seed(req.seed)
+    lt = (screen.LooseTightJK(opt, None, loose, switch, max_loose, mixed_threshold)
+          if loose_tight else None)
     out = []
     prev = jacc = kacc = None
     for c in range(req.cycles):
-        if incremental and c % max(1, int(rebuild_every)) != 0:
+        if lt is not None:
+            jacc, kacc = lt.jk(d)
+        elif incremental and c % max(1, int(rebuild_every)) != 0:
             vj, vk = opt.get_jk(d - prev, 1, mixed_threshold=mixed_threshold)
             jacc, kacc = jacc + vj, kacc + vk
         else:
@@ -299,5 +331,5 @@ def serve_alone(req: Request, device: int | None = None, mixed_threshold: float 
         prev = d.clone()
         out.append((jacc.cpu().numpy(), kacc.cpu().numpy()))
         if c + 1 < req.cycles:
-            advance_density(d, req.sigma, gen)
+            advance_density(d, req.sigma * req.sigma_decay ** c, gen)
     return out

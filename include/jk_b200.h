@@ -207,6 +207,18 @@ int jk_plan_memory(const jk_plan *plan, long long *table_bytes,
 int jk_plan_set_shard(jk_plan *plan, int rank, int size);
 
 /*
+ * Screening threshold of the plan's later builds (single and batched):
+ * quartets are kept when q_ij + q_kl + log max|D| > log(tol).  tol must be
+ * at least the plan's direct_scf_tol (its pair lists hold only the pairs
+ * that threshold can need); tol equal to it restores the default.  The
+ * counterpart of raising _VHFOpt.direct_scf_tol between builds, which the
+ * reference's loose-then-tight SCF screening does for its loose cycles
+ * (electrolites/fastscfscreen.py:107-118; the builds read the attribute at
+ * call time).
+ */
+int jk_plan_set_tol(jk_plan *plan, double tol);
+
+/*
  * Per-class launch tuning of the plan's builds: the number of tasks per SM
  * the task size aims at, a cap on resident blocks per SM (0: the occupancy
  * limit), and whether mixed-precision builds may run this class's

@@ -185,9 +185,9 @@ struct Engine {
         cls_maxprim[JK_NCLASSES];
     int cls_nlaunch[JK_NCLASSES], cls_cnt0[JK_NCLASSES];   // launches per class, first counter
     int ncounters = 0;
-    size_t off_views = 0, off_row0 = 0, off_pre = 0, off_post = 0, off_cond = 0;
-    int npre = 0, npost = 0;
-    long long pre_tiles = 0, post_tiles = 0, cond_blocks = 0;
+    size_t off_views = 0, off_row0 = 0, off_pre = 0, off_post = 0, off_cond = 0, off_pair = 0;
+    int npre = 0, npost = 0, npair = 0;
+    long long pre_tiles = 0, post_tiles = 0, cond_blocks = 0, pair_blocks = 0;
     char *ws = nullptr;             // workspace of the prepared build
     size_t acc_bytes = 0;           // accumulators at its start (cleared per build)
 };
@@ -371,6 +371,8 @@ struct Item {
     int n_k = 0, n_j = 0, n_ka = 0;
     bool need_t = false;
     double *Kh = nullptr, *Jh = nullptr, *dsJ = nullptr, *DT = nullptr;
+    double2 *dmK2 = nullptr;        // K densities interleaved in pairs
+    int n_kp = 0;                   // pairs of them (0: not interleaved)
     float *dmc = nullptr, *dm_max = nullptr;
 };
 
@@ -421,6 +423,8 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     const int n = (int)items.size();
     if (n <= 0) return fail(JK_ERR_ARG, std::string(who) + ": no items");
     // ---- workspace: accumulators of every item, then per-item buffers ----
+    // (the library's static scratch of jk_build_noalloc holds no pair copies)
+    const bool pair_k = ws_ext == nullptr;
     size_t acc = 0, need = 0;
     for (int i = 0; i < n; ++i) {
         Item &it = items[i];
@@ -436,6 +440,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         it.n_j = (s.with_j && s.hermi != 2) ? it.n_dm : 0;
         it.n_ka = it.n_k ? it.n_dm : 0;
         it.need_t = s.with_k && s.hermi == 0;
+        it.n_kp = pair_k ? it.n_k / 2 : 0;
         acc += align256((size_t)it.n_k * nao2 * 8) + align256((size_t)it.n_j * nao2 * 8);
     }
     need = acc;
@@ -443,6 +448,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         const size_t nao2 = (size_t)it.p->nao * it.p->nao;
         need += align256((size_t)it.n_j * nao2 * 8) +
                 align256(it.need_t ? (size_t)it.n_dm * nao2 * 8 : 0) +
+                align256((size_t)it.n_kp * nao2 * 16) +
                 align256((size_t)it.p->nbas * it.p->nbas * 4);
     }
     need += align256((size_t)n * 4);
@@ -485,6 +491,8 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         o += align256((size_t)it.n_j * nao2 * 8);
         it.DT = (double *)(ws + o);
         o += align256(it.need_t ? (size_t)it.n_dm * nao2 * 8 : 0);
+        it.dmK2 = it.n_kp ? (double2 *)(ws + o) : nullptr;
+        o += align256((size_t)it.n_kp * nao2 * 16);
         it.dmc = (float *)(ws + o);
         o += align256((size_t)it.p->nbas * it.p->nbas * 4);
     }
@@ -531,6 +539,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             v.dm_max = it.dm_max;
             v.dmK = it.dm;
             v.dmKT = it.DT;
+            v.dmK2 = it.dmK2;
             v.dsJ = it.dsJ;
             v.Kh = it.Kh;
             v.Jh = it.Jh;
@@ -581,7 +590,8 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     // ---- density preparation, screening and assembly descriptors ----
     std::vector<TileOp> pre, post;
     std::vector<CondItem> cond;
-    long long pre_tiles = 0, post_tiles = 0, cblk = 0;
+    std::vector<PairOp> pairs;
+    long long pre_tiles = 0, post_tiles = 0, cblk = 0, pblk = 0;
     auto op = [](const double *a, const double *b, double *out, double *outT, double f, int nao,
                  int nd, long long &tiles) {
         TileOp t;
@@ -631,11 +641,25 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         ci.pad = 0;
         cblk += (long long)ci.nt * ci.nt;
         cond.push_back(ci);
+        // K density d is dm[d] for d < n_ka, then the transposes DT[d - n_ka]
+        auto kd = [&](int d) { return d < it.n_ka ? it.dm + d * nao2 : it.DT + (d - it.n_ka) * nao2; };
+        for (int q = 0; q < it.n_kp; ++q) {
+            PairOp po;
+            po.a = kd(2 * q);
+            po.b = kd(2 * q + 1);
+            po.out = it.dmK2 + q * nao2;
+            po.n = (long long)nao2;
+            po.blk0 = pblk;
+            pblk += ((long long)nao2 + JK_PAIR_THREADS - 1) / JK_PAIR_THREADS;
+            pairs.push_back(po);
+        }
     }
-    if (pre_tiles > INT_MAX || post_tiles > INT_MAX || cblk > INT_MAX)
+    if (pre_tiles > INT_MAX || post_tiles > INT_MAX || cblk > INT_MAX || pblk > INT_MAX)
         return fail(JK_ERR_ARG, std::string(who) + ": build too large");
     E.npre = (int)pre.size();
     E.npost = (int)post.size();
+    E.npair = (int)pairs.size();
+    E.pair_blocks = pblk;
     E.pre_tiles = pre_tiles;
     E.post_tiles = post_tiles;
     E.cond_blocks = cblk;
@@ -644,13 +668,15 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     E.off_pre = E.off_row0 + align256(row0.size() * sizeof(int));
     E.off_post = E.off_pre + align256(pre.size() * sizeof(TileOp));
     E.off_cond = E.off_post + align256(post.size() * sizeof(TileOp));
-    const size_t total = E.off_cond + align256(cond.size() * sizeof(CondItem));
+    E.off_pair = E.off_cond + align256(cond.size() * sizeof(CondItem));
+    const size_t total = E.off_pair + align256(pairs.size() * sizeof(PairOp));
     E.blob.assign(total, 0);
     put(E.blob, E.off_views, views);
     put(E.blob, E.off_row0, row0);
     put(E.blob, E.off_pre, pre);
     put(E.blob, E.off_post, post);
     put(E.blob, E.off_cond, cond);
+    put(E.blob, E.off_pair, pairs);
     RC(engine_reserve_rows(E, std::max<long long>(1, max_rows), no_alloc, who));
     RC(engine_reserve_blob(E, total, no_alloc, who));
     return JK_OK;
@@ -755,6 +781,12 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
     dm_max_kernel<<<E.nitems, 256, 0, st>>>(d_cond, E.d_error);
     CK(cudaGetLastError());
     E.launches += 2;
+    if (E.npair) {   // after the transposes of the pre step
+        pair_dens_kernel<<<(unsigned)E.pair_blocks, JK_PAIR_THREADS, 0, st>>>(
+            (const PairOp *)(E.d_blob + E.off_pair), E.npair);
+        CK(cudaGetLastError());
+        E.launches++;
+    }
     if (E.ncounters) CK(cudaMemsetAsync(E.d_counters, 0, E.ncounters * sizeof(int), st));
     CK(cudaMemsetAsync(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
     char msg[256] = {0};

@@ -54,6 +54,9 @@ struct PlanView {
     // non-hermitian builds).  J reads dsJ[0..n_j) = D + D^T.
     const double *dmK;
     const double *dmKT;
+    // the K densities interleaved in pairs (2p, 2p+1), p < n_k / 2, for the
+    // register digest (null: every density read on its own)
+    const double2 *dmK2;
     const double *dsJ;
     double *Kh;              // half-K accumulators (n_k, nao, nao)
     double *Jh;              // half-J accumulators (n_j, nao, nao)

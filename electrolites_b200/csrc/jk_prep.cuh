@@ -196,6 +196,32 @@ struct TileOp {
     long long tile0;    // first block of this op in the launch
 };
 
+// Two densities interleaved element by element, out[i] = (a[i], b[i]): the
+// register digest of a build with two or more K densities reads both
+// densities of a pair with one 16-byte load.
+struct PairOp {
+    const double *a;
+    const double *b;
+    double2 *out;
+    long long n;        // elements of one density (nao^2)
+    long long blk0;     // first block of this op in the launch
+};
+
+#define JK_PAIR_THREADS 256
+
+__global__ void pair_dens_kernel(const PairOp *__restrict__ ops, int nops)
+{
+    const long long blk = blockIdx.x;
+    int lo = 0, hi = nops - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ops[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
+    }
+    const PairOp o = ops[lo];
+    const long long i = (blk - o.blk0) * JK_PAIR_THREADS + threadIdx.x;
+    if (i < o.n) o.out[i] = make_double2(o.a[i], o.b[i]);
+}
+
 __global__ void tile_op_kernel(const TileOp *__restrict__ ops, int nops)
 {
     __shared__ double tile[32][33];

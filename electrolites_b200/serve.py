@@ -77,9 +77,10 @@ class Request:
 def matrix_bytes(nao: int, nbas: int, n_dm: int, incremental: bool = False) -> int:
     """Device bytes of a request's matrices: densities, J, K, and its share
     of the build workspace (half-J/K accumulators, symmetrised densities,
-    screening table) for hermi = 1; incremental mode keeps four more (the
-    previous density, the density change, accumulated J and K)."""
-    return 8 * nao * nao * n_dm * (3 + 3 + (4 if incremental else 0)) + 4 * nbas * nbas
+    the pair-interleaved copy of the K densities, screening table) for
+    hermi = 1; incremental mode keeps four more (the previous density, the
+    density change, accumulated J and K)."""
+    return 8 * nao * nao * n_dm * (3 + 4 + (4 if incremental else 0)) + 4 * nbas * nbas
 
 
 def table_bound(nbas: int) -> int:

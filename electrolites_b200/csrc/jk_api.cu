@@ -719,6 +719,10 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     a.mixed_tab = 0;
     a.shard_rank = E.shard_rank;
     a.shard_size = E.shard_size;
+    // batched register-form classes take a bra's sub-lists as one task range
+    // (the batched kernel walks them); a single plan's keep per-sub-list
+    // tasks, whose count fills the GPU for a small molecule
+    a.grouped = jk_class_table[c].form == 0 && E.cls_nview[c] > 1;
     a.nterm = E.nterm;
     for (int t = 0; t < 2; ++t) {
         a.op_coef[t] = E.op_coef[t];
@@ -829,8 +833,8 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
         CK(cub::DeviceScan::InclusiveSum(cub, tmp, rb, cand_prefix, rows, cst));
         const int lo = ce.form == 0 ? 128 : 32, hi = ce.form == 0 ? 4096 : 1024;
         const int target = std::max(1, E.tune[c].tasks_per_sm) * E.num_sms;
-        task_chunks_kernel<<<(rows + 255) / 256, 256, 0, cst>>>(rb, cand_prefix, rows, target, lo,
-                                                                hi, E.d_chunk + c, chunks);
+        task_chunks_kernel<<<(rows + 255) / 256, 256, 0, cst>>>(a, rb, cand_prefix, rows, target,
+                                                                lo, hi, E.d_chunk + c, chunks);
         CK(cudaGetLastError());
         tmp = E.cub_bytes;
         CK(cub::DeviceScan::InclusiveSum(cub, tmp, chunks, prefix, rows, cst));

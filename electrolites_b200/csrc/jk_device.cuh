@@ -81,6 +81,10 @@ struct ClassArgs {
     int mixed;               // 1: the build has FP32 quartets (mixed form)
     int mixed_tab;           // 1: the FP32 Rys table is in shared memory (set at launch)
     int shard_rank, shard_size;   // this GPU takes tasks t = rank mod size
+    // 1: a task is a range of the concatenated candidate kets of all ket
+    // sub-lists of one bra pair (its chunks are counted on the bra's first
+    // row), so a warp's queue runs on across sub-lists; 0: one sub-list's
+    int grouped;
     // the operator: sum over nterm (1 or 2) terms of op_coef[t] times the
     // Coulomb operator (op_inv_om2[t] = 0) or the long-range erf(omega r)/r
     // (op_inv_om2[t] = 1/omega^2); quartets are screened by the Coulomb bound

@@ -361,9 +361,12 @@ __global__ void task_rows_kernel(const ClassArgs a, int *__restrict__ row_ncand)
 
 // Task size from the class's total candidate count (cand_prefix[rows-1]):
 // about `target` tasks, clamped to [lo, hi] kets and rounded to a warp; then
-// the chunk count of every row.
-__global__ void task_chunks_kernel(const int *__restrict__ ncand, const int *__restrict__ cand_prefix,
-                                   int rows, int target, int lo, int hi, int *__restrict__ chunk_out,
+// the chunk count of every row.  Grouped classes (a.grouped) count the
+// chunks of a bra pair's candidates over all its ket sub-lists on the bra's
+// first row (sub-list 0) and none on its other rows.
+__global__ void task_chunks_kernel(const ClassArgs a, const int *__restrict__ ncand,
+                                   const int *__restrict__ cand_prefix, int rows, int target,
+                                   int lo, int hi, int *__restrict__ chunk_out,
                                    int *__restrict__ chunks)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -373,5 +376,22 @@ __global__ void task_chunks_kernel(const int *__restrict__ ncand, const int *__r
     if (c < lo) c = lo;
     if (c > hi) c = hi;
     if (r == 0) *chunk_out = (int)c;
-    if (r < rows) chunks[r] = (int)((ncand[r] + c - 1) / c);
+    if (r >= rows) return;
+    if (!a.grouped) {
+        chunks[r] = (int)((ncand[r] + c - 1) / c);
+        return;
+    }
+    int vlo = 0, vhi = a.nviews - 1;
+    while (vlo < vhi) {                  // last view with row0 <= r
+        const int mid = (vlo + vhi + 1) >> 1;
+        if (a.view_row0[mid] <= r) vlo = mid; else vhi = mid - 1;
+    }
+    const PlanView &V = a.views[vlo];
+    const int s = (r - V.row0) % V.nsub;
+    if (s != 0) {
+        chunks[r] = 0;
+        return;
+    }
+    const long long g = cand_prefix[r + V.nsub - 1] - (r > 0 ? cand_prefix[r - 1] : 0);
+    chunks[r] = (int)((g + c - 1) / c);
 }

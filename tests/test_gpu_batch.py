@@ -234,3 +234,33 @@ def test_one_or_two_class_streams_agree(torch, opts):
     o.set_timing(False)
     assert ms and launches > 0
     assert _maxdiff(a[0], b[0]) <= 1e-12 and _maxdiff(a[1], b[1]) <= 1e-12
+
+
+def test_grouped_tasks_split_and_single_view_launch(torch):
+    """Batched register-form tasks cover a bra pair's candidates over all its
+    ket sub-lists.  A (H2O)_12 member with the smallest task size splits
+    those ranges over several tasks; 193 molecules put 193 views in every
+    class, so each class's second launch holds one view and still runs the
+    batched (grouped) kernel.  Both equal one build per molecule (1e-10)."""
+    from electrolites_b200.batch import JKBatch
+    from electrolites_b200.jk import VHFOpt, class_keys
+    mols = [clusters.water_mole(12, 8.0, 31, basis='6-31g*'),
+            clusters.water_mole(1, 3.0, 32, basis='6-31g*'),
+            clusters.water_mole(3, 4.5, 33, basis='def2-svp')]
+    plans = [VHFOpt(m, 1e-13).build() for m in mols]
+    dms = [torch.as_tensor(dens_stack(m, 2, 1, 40 + i), device='cuda') for i, m in enumerate(mols)]
+    batch = JKBatch()
+    for c in range(len(class_keys())):
+        batch.set_tuning(c, 4096)          # many tasks: the smallest task size
+    vj, vk = batch.build(plans, dms, 1)
+    ref = _single(torch, plans, dms, 1)
+    for i in range(len(mols)):
+        assert _maxdiff(vj[i], ref[i][0]) <= ATOL
+        assert _maxdiff(vk[i], ref[i][1]) <= ATOL
+    mols = [clusters.water_mole(1, 3.0, 100 + i, basis='6-31g*') for i in range(193)]
+    plans = [VHFOpt(m, 1e-13).build() for m in mols]
+    dms = [torch.as_tensor(dens_stack(m, 1, 1, i), device='cuda') for i, m in enumerate(mols)]
+    vj, vk = JKBatch().build(plans, dms, 1)
+    for i in (0, 100, 191, 192):
+        rj, rk = plans[i].get_jk(dms[i], 1)
+        assert _maxdiff(vj[i], rj) <= ATOL and _maxdiff(vk[i], rk) <= ATOL

@@ -20,7 +20,7 @@ EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_build_host', 'jk_sync', 'jk_last_counts', 'jk_class_info',
            'jk_set_timing', 'jk_last_class_ms', 'jk_fp64_peak', 'jk_build_noalloc',
            'jk_plan_q_cond', 'jk_build_rs', 'jk_build_op', 'jk_plan_memory', 'jk_plan_set_shard',
-           'jk_plan_set_tol', 'jk_plan_set_tuning',
+           'jk_plan_set_tol', 'jk_plan_set_jengine', 'jk_plan_set_tuning',
            'jk_batch_create', 'jk_batch_destroy', 'jk_batch_build', 'jk_batch_sync',
            'jk_batch_counts', 'jk_batch_set_timing', 'jk_batch_class_ms',
            'jk_batch_set_tuning', 'jk_batch_stats', 'jk_last_error']
@@ -69,6 +69,7 @@ def lib():
     L.jk_plan_memory.argtypes = [vp, llp, llp]
     L.jk_plan_set_shard.argtypes = [vp, c_int, c_int]
     L.jk_plan_set_tol.argtypes = [vp, c_double]
+    L.jk_plan_set_jengine.argtypes = [vp, c_int]
     L.jk_plan_set_tuning.argtypes = [vp, c_int, c_int, c_int, c_int]
     L.jk_batch_create.argtypes = [c_int, ctypes.POINTER(vp)]
     L.jk_batch_destroy.argtypes = [vp]

@@ -346,14 +346,17 @@ def gen_class_header(cls):
 
 
 def gen_unit(A, B, cls):
-    return '\n'.join([
-        '// Generated by electrolites_b200/codegen/gen_classes.py -- do not edit.',
-        '#include "../jk_kernels.cuh"',
-        '',
-        gen_class_header(cls),
-        '',
-        f'JK_DEFINE_CLASS({cls.tag}, {A}, {B})',
-        ''])
+    lines = ['// Generated by electrolites_b200/codegen/gen_classes.py -- do not edit.',
+             '#include "../jk_kernels.cuh"',
+             '',
+             gen_class_header(cls),
+             '',
+             f'JK_DEFINE_CLASS({cls.tag}, {A}, {B})']
+    if cls.lk == 0 and cls.ll == 0:
+        # (la lb|ss): its bra transfer is the pair class's, for the J engine
+        lines.append(f'JK_DEFINE_PAIR({cls.tag})')
+    lines.append('')
+    return '\n'.join(lines)
 
 
 def write_all(outdir, lmax=LMAX):
@@ -387,6 +390,18 @@ def write_all(outdir, lmax=LMAX):
         reg.append(f'    {{{A}, {B}, {cls.li}, {cls.lj}, {cls.lk}, {cls.ll}, '
                    f'{form}, {1 if cls.form == "reg" else cls.team_threads}, {fp32}, '
                    f'jk_launch_{cls.tag}}},')
+    reg.append('};')
+    # J engine: pair transforms per pair class, from the (la lb|ss) units
+    pairs = [(A, cls) for A, B, cls in classes if cls.lk == 0 and cls.ll == 0]
+    pairs.sort(key=lambda t: t[0])
+    for A, cls in pairs:
+        reg.append(f'int jk_pair_dens_{cls.tag}(const PairArgs &a, cudaStream_t st);')
+        reg.append(f'int jk_pair_post_{cls.tag}(const PairArgs &a, cudaStream_t st);')
+    reg.append(f'#define JK_NPAIR_TABLE {len(pairs)}')
+    reg.append('static const PairEntry jk_pair_table[JK_NPAIR_TABLE] = {')
+    for A, cls in pairs:
+        reg.append(f'    {{{A}, {cls.li}, {cls.lj}, {cls.ne}, jk_pair_dens_{cls.tag}, '
+                   f'jk_pair_post_{cls.tag}}},')
     reg.append('};')
     with open(os.path.join(outdir, 'class_table.inc.tmp'), 'w') as f:
         f.write('\n'.join(reg) + '\n')

@@ -171,6 +171,13 @@ struct Engine {
     // erf(omega_t r)/r with op_inv_om2[t] = 1/omega_t^2)
     int nterm = 1;
     double op_coef[2] = {1.0, 0.0}, op_inv_om2[2] = {0.0, 0.0};
+    // J engine of the prepared build (one plan, J only)
+    int jx = 0;
+    double *jx_dens = nullptr, *jx_acc = nullptr;
+    const jk_plan *jx_plan = nullptr;
+    const double *jx_ds = nullptr;
+    double *jx_Jh = nullptr;
+    int jx_nj = 0;
     bool timing = false;
     std::vector<cudaEvent_t> ev;    // 2 per class
     std::vector<char> ev_used;
@@ -223,6 +230,8 @@ struct jk_plan {
     int2 *d_subs = nullptr;
     double *d_io = nullptr;         // device buffers of jk_build_host
     size_t io_size = 0;
+    long long nx_total = 0;         // x-space elements per density (J engine)
+    bool jengine = true;            // J-only builds through the J engine
     Engine eng;                     // the plan's own builds
 };
 
@@ -425,6 +434,9 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     // ---- workspace: accumulators of every item, then per-item buffers ----
     // (the library's static scratch of jk_build_noalloc holds no pair copies)
     const bool pair_k = ws_ext == nullptr;
+    // J engine: a J-only build of one plan outside the static scratch
+    const bool jx = n == 1 && items[0].p && items[0].p->jengine && s.with_j && !s.with_k &&
+                    s.hermi != 2 && s.nterm == 1 && ws_ext == nullptr;
     size_t acc = 0, need = 0;
     for (int i = 0; i < n; ++i) {
         Item &it = items[i];
@@ -443,7 +455,9 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         it.n_kp = pair_k ? it.n_k / 2 : 0;
         acc += align256((size_t)it.n_k * nao2 * 8) + align256((size_t)it.n_j * nao2 * 8);
     }
-    need = acc;
+    const size_t jx_bytes = jx ? align256((size_t)items[0].n_j * items[0].p->nx_total * 8) : 0;
+    acc += jx_bytes;               // the x-space J, cleared with the accumulators
+    need = acc + jx_bytes;         // and the x-space densities
     for (const Item &it : items) {
         const size_t nao2 = (size_t)it.p->nao * it.p->nao;
         need += align256((size_t)it.n_j * nao2 * 8) +
@@ -485,6 +499,9 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         it.Jh = (double *)(ws + o);
         o += align256((size_t)it.n_j * nao2 * 8);
     }
+    E.jx = jx;
+    E.jx_acc = jx ? (double *)(ws + o) : nullptr;
+    o += jx_bytes;
     for (Item &it : items) {
         const size_t nao2 = (size_t)it.p->nao * it.p->nao;
         it.dsJ = (double *)(ws + o);
@@ -495,6 +512,14 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         o += align256((size_t)it.n_kp * nao2 * 16);
         it.dmc = (float *)(ws + o);
         o += align256((size_t)it.p->nbas * it.p->nbas * 4);
+    }
+    E.jx_dens = jx ? (double *)(ws + o) : nullptr;
+    o += jx_bytes;
+    if (jx) {
+        E.jx_plan = items[0].p;
+        E.jx_ds = items[0].dsJ;
+        E.jx_Jh = items[0].Jh;
+        E.jx_nj = items[0].n_j;
     }
     float *dm_max = (float *)(ws + o);
     for (int i = 0; i < n; ++i) items[i].dm_max = dm_max + i;
@@ -723,6 +748,9 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     // (the batched kernel walks them); a single plan's keep per-sub-list
     // tasks, whose count fills the GPU for a small molecule
     a.grouped = jk_class_table[c].form == 0 && E.cls_nview[c] > 1;
+    a.jx = E.jx;
+    a.jx_dens = E.jx_dens;
+    a.jx_acc = E.jx_acc;
     a.nterm = E.nterm;
     for (int t = 0; t < 2; ++t) {
         a.op_coef[t] = E.op_coef[t];
@@ -765,6 +793,31 @@ static int engine_configure(Engine &E)
     return JK_OK;
 }
 
+// J engine: the pair transforms of every pair class of the build's plan,
+// densities (post = false) or J (post = true)
+static int jx_pairs(Engine &E, cudaStream_t st, bool post)
+{
+    const jk_plan *p = E.jx_plan;
+    for (int t = 0; t < JK_NPAIR_TABLE; ++t) {
+        const PairEntry &pe = jk_pair_table[t];
+        PairArgs a;
+        a.pairs = p->d_pairs + p->pc_off[pe.pair_class];
+        a.npairs = p->pc_off[pe.pair_class + 1] - p->pc_off[pe.pair_class];
+        if (a.npairs == 0) continue;
+        a.n_j = E.jx_nj;
+        a.nao = p->nao;
+        a.ds = E.jx_ds;
+        a.Jh = E.jx_Jh;
+        a.dt = E.jx_dens;
+        a.jx = E.jx_acc;
+        const int rc = post ? pe.post(a, st) : pe.dens(a, st);
+        if (rc) return fail(JK_ERR_CUDA, std::string("J engine pair kernel: ") +
+                                             cudaGetErrorString((cudaError_t)rc));
+        E.launches++;
+    }
+    return JK_OK;
+}
+
 // The launch stream of a prepared build (stream operations only, so that it
 // can be captured).
 static int engine_launch(Engine &E, cudaStream_t st, bool timing)
@@ -791,6 +844,7 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
         CK(cudaGetLastError());
         E.launches++;
     }
+    if (E.jx) RC(jx_pairs(E, st, false));   // x-space densities of every pair
     if (E.ncounters) CK(cudaMemsetAsync(E.d_counters, 0, E.ncounters * sizeof(int), st));
     CK(cudaMemsetAsync(E.d_nq, 0, 3 * JK_NCLASSES * sizeof(unsigned long long), st));
     char msg[256] = {0};
@@ -863,6 +917,7 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
         CK(cudaEventRecord(E.ev_join[s - 1], cs[s]));
         CK(cudaStreamWaitEvent(st, E.ev_join[s - 1], 0));
     }
+    if (E.jx) RC(jx_pairs(E, st, true));    // x-space J into the half-J accumulators
     if (E.npost) {
         tile_op_kernel<<<(unsigned)E.post_tiles, dim3(32, 8), 0, st>>>(d_post, E.npost);
         CK(cudaGetLastError());
@@ -1165,7 +1220,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
             r.prim0 = cand[c].z;
             r.nprim = cand[c].w;
             r.q = q[c];
-            r.pad = 0.f;
+            r.xoff = 0;       // set below, once the classes are laid out
             r.ABx = shells[i].x - shells[j].x;
             r.ABy = shells[i].y - shells[j].y;
             r.ABz = shells[i].z - shells[j].z;
@@ -1175,6 +1230,21 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
         p->pc_maxprim[k] = mp;
     }
     p->pc_off[NPAIR_CLASSES] = (int)recs.size();
+    // x-space blocks of the J engine in pair order: NX = sum of ncart over
+    // the transfer's source levels la..la+lb
+    long long xo = 0;
+    for (int la = 0; la < 4; ++la)
+        for (int lb = 0; lb <= la; ++lb) {
+            const int k = pair_class(la, lb);
+            int nx = 0;
+            for (int L = la; L <= la + lb; ++L) nx += ncart(L);
+            for (int r = p->pc_off[k]; r < p->pc_off[k + 1]; ++r) {
+                recs[r].xoff = (int)xo;
+                xo += nx;
+            }
+        }
+    if (xo > INT_MAX / 8) return fail(JK_ERR_ARG, "molecule too large (J engine blocks)");
+    p->nx_total = xo;
     for (int k = 0; k < NPAIR_CLASSES; ++k)   // kernels queue ket indices in 28 bits
         if (p->pc_off[k + 1] - p->pc_off[k] >= (1 << 28))
             return fail(JK_ERR_ARG, "molecule too large (shell pairs of one class)");
@@ -1270,6 +1340,13 @@ extern "C" int jk_plan_set_shard(jk_plan *plan, int rank, int size)
         return fail(JK_ERR_ARG, "jk_plan_set_shard: need 0 <= rank < size");
     plan->eng.shard_rank = rank;
     plan->eng.shard_size = size;
+    return JK_OK;
+}
+
+extern "C" int jk_plan_set_jengine(jk_plan *plan, int on)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_jengine: plan is NULL");
+    plan->jengine = on != 0;
     return JK_OK;
 }
 

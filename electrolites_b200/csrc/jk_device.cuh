@@ -12,6 +12,10 @@
 //   q                  float log(sqrt(max_ab |(ab|ab)|)) per pair record.
 //   dm_cond            float log(max |D| over densities, both orientations)
 //                      per shell pair, nbas x nbas.
+//   x-space blocks     J engine: per shell pair P of class (la, lb), n_j x
+//                      NX doubles, NX = sum_{L=la}^{la+lb} ncart(L) (the
+//                      source levels of the pair's transfer H^P):
+//                      D~_P = H^P^T (D+D^T)_P and the x-space J of P.
 //   densities / J / K  double (n, nao, nao), row-major, Cartesian AO order.
 #pragma once
 #include <cstdint>
@@ -35,7 +39,7 @@ struct PairRec {
     int i0, j0;          // first Cartesian AO of each shell
     int prim0, nprim;    // first record and count in the prim-pair table
     float q;             // log Schwarz bound
-    float pad;
+    int xoff;            // first element of this pair's x-space block (J engine)
     double ABx, ABy, ABz;  // A - B, for the i -> j transfer
 };
 
@@ -91,6 +95,13 @@ struct ClassArgs {
     int nterm;
     double op_coef[2];
     double op_inv_om2[2];
+    // J engine (J-only single-plan builds): 1 = contract each quartet's
+    // (e0|f0) block with the pairs' x-space densities instead of
+    // transferring it to (ij|kl); pair P's block of n_j x NX(P) doubles
+    // starts at P.xoff * n_j in jx_dens (densities) and jx_acc (J)
+    int jx;
+    const double *jx_dens;
+    double *jx_acc;
     const double *rys;       // Rys table (double): polynomial part + large-x
     const float *rys32;      // Rys table (float)
     int *counter;            // task counter of this launch

@@ -26,3 +26,22 @@ struct ClassEntry {
     int fp32_default;             // mixed builds run FP32 quartets here by default
     ClassLauncher launch;
 };
+
+// J engine, per pair class: the x-space densities D~_P = H^P^T (D+D^T)_P of
+// every pair of the class, and the transfer of their x-space J back into the
+// half-J accumulators, J_h(P) += H^P J~_P (one thread per pair and density).
+struct PairArgs {
+    const PairRec *pairs;         // the class's pairs
+    int npairs;
+    int n_j, nao;
+    const double *ds;             // D + D^T, n_j x nao x nao
+    double *Jh;                   // half-J accumulators, n_j x nao x nao
+    double *dt;                   // x-space densities
+    const double *jx;             // x-space J
+};
+typedef int (*PairLauncher)(const PairArgs &a, cudaStream_t st);
+
+struct PairEntry {
+    int pair_class, la, lb, nx;
+    PairLauncher dens, post;
+};

@@ -111,6 +111,12 @@ class VHFOpt:
             self.build()
         return self._plan
 
+    def set_jengine(self, on=True):
+        """J-only builds through the J engine (default) or the (ij|kl)
+        digest of J/K builds; the same J to rounding."""
+        _lib.check(_lib.lib().jk_plan_set_jengine(self.plan, int(bool(on))),
+                   'jk_plan_set_jengine')
+
     def apply_tol(self):
         """Hands ``direct_scf_tol`` to the plan if it changed since the last
         build: builds read it at call time, as the reference's do.  A value

@@ -219,6 +219,21 @@ int jk_plan_set_shard(jk_plan *plan, int rank, int size);
 int jk_plan_set_tol(jk_plan *plan, double tol);
 
 /*
+ * J engine of the plan's J-only builds (with_j = 1, with_k = 0; on by
+ * default): each quartet's (e0|f0) block is contracted with the pairs'
+ * x-space densities D~ = H^T (D + D^T) (H: a pair's horizontal transfer)
+ * instead of being transferred to (ij|kl) and digested; the x-space J of
+ * every pair is transferred back once per build.  Same quartets, same
+ * screening, same result to rounding; off (on = 0), J-only builds digest
+ * (ij|kl) like J/K builds.  The counterpart of the reference's J engine
+ * for J-only builds, j_engine._VHFOpt.get_j (electrolites/fastj.py:540-569,
+ * McMurchie-Davidson over Hermite densities; here the density contraction
+ * happens in the Rys transfer's source space).  Batched and jk_build_noalloc
+ * builds use the (ij|kl) digest.
+ */
+int jk_plan_set_jengine(jk_plan *plan, int on);
+
+/*
  * Per-class launch tuning of the plan's builds: the number of tasks per SM
  * the task size aims at, a cap on resident blocks per SM (0: the occupancy
  * limit), and whether mixed-precision builds may run this class's

@@ -173,6 +173,7 @@ struct Engine {
     double op_coef[2] = {1.0, 0.0}, op_inv_om2[2] = {0.0, 0.0};
     // J engine of the prepared build (one plan, J only)
     int jx = 0;
+    bool jx_jonly = false;          // the J engine's build has no K
     double *jx_dens = nullptr, *jx_acc = nullptr;
     const jk_plan *jx_plan = nullptr;
     const double *jx_ds = nullptr;
@@ -434,9 +435,10 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     // ---- workspace: accumulators of every item, then per-item buffers ----
     // (the library's static scratch of jk_build_noalloc holds no pair copies)
     const bool pair_k = ws_ext == nullptr;
-    // J engine: a J-only build of one plan outside the static scratch
-    const bool jx = n == 1 && items[0].p && items[0].p->jengine && s.with_j && !s.with_k &&
-                    s.hermi != 2 && s.nterm == 1 && ws_ext == nullptr;
+    // J engine: J of a one-plan, one-operator build outside the static
+    // scratch (with K: the quartets kept for J alone)
+    const bool jx = n == 1 && items[0].p && items[0].p->jengine && s.with_j && s.hermi != 2 &&
+                    s.nterm == 1 && ws_ext == nullptr;
     size_t acc = 0, need = 0;
     for (int i = 0; i < n; ++i) {
         Item &it = items[i];
@@ -500,6 +502,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         o += align256((size_t)it.n_j * nao2 * 8);
     }
     E.jx = jx;
+    E.jx_jonly = !s.with_k;
     E.jx_acc = jx ? (double *)(ws + o) : nullptr;
     o += jx_bytes;
     for (Item &it : items) {
@@ -748,7 +751,9 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     // (the batched kernel walks them); a single plan's keep per-sub-list
     // tasks, whose count fills the GPU for a small molecule
     a.grouped = jk_class_table[c].form == 0 && E.cls_nview[c] > 1;
-    a.jx = E.jx;
+    // the J engine: every class of a J-only build; with K, the team-form
+    // classes (J from the x-space contraction, K from the transfers)
+    a.jx = E.jx && (E.jx_jonly || jk_class_table[c].form == 1);
     a.jx_dens = E.jx_dens;
     a.jx_acc = E.jx_acc;
     a.nterm = E.nterm;

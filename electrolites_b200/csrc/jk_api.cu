@@ -174,6 +174,7 @@ struct Engine {
     // J engine of the prepared build (one plan, J only)
     int jx = 0;
     bool jx_jonly = false;          // the J engine's build has no K
+    bool jx_reg = true;             // J/K builds: register-form classes too
     double *jx_dens = nullptr, *jx_acc = nullptr;
     const jk_plan *jx_plan = nullptr;
     const double *jx_ds = nullptr;
@@ -753,7 +754,7 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     a.grouped = jk_class_table[c].form == 0 && E.cls_nview[c] > 1;
     // the J engine: every class of a J-only build; with K, the team-form
     // classes (J from the x-space contraction, K from the transfers)
-    a.jx = E.jx && (E.jx_jonly || jk_class_table[c].form == 1);
+    a.jx = E.jx && (E.jx_jonly || jk_class_table[c].form == 1 || E.jx_reg);
     a.jx_dens = E.jx_dens;
     a.jx_acc = E.jx_acc;
     a.nterm = E.nterm;

@@ -219,12 +219,11 @@ int jk_plan_set_shard(jk_plan *plan, int rank, int size);
 int jk_plan_set_tol(jk_plan *plan, double tol);
 
 /*
- * J engine of the plan's builds (on by default): in J-only builds (with_j =
- * 1, with_k = 0) every class, in J/K builds the team-form classes, contract
- * each quartet's (e0|f0) block with the pairs'
+ * J engine of the plan's builds (on by default): J of every quartet from its
+ * (e0|f0) block contracted with the pairs'
  * x-space densities D~ = H^T (D + D^T) (H: a pair's horizontal transfer)
- * instead of being transferred to (ij|kl) and digested; the x-space J of
- * every pair is transferred back once per build.  Same quartets, same
+ * instead of the (ij|kl) digest (K, if asked for, still from (ij|kl)); the
+ * x-space J of every pair is transferred back once per build.  Same quartets, same
  * screening, same result to rounding; off (on = 0), J is digested from
  * (ij|kl).  The counterpart of the reference's J engine
  * for J-only builds, j_engine._VHFOpt.get_j (electrolites/fastj.py:540-569,

@@ -1249,7 +1249,11 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
                 xo += nx;
             }
         }
-    if (xo > INT_MAX / 8) return fail(JK_ERR_ARG, "molecule too large (J engine blocks)");
+    if (xo > INT_MAX / 8) {   // beyond the J engine's block indices: J from (ij|kl)
+        for (PairRec &r : recs) r.xoff = 0;
+        xo = 0;
+        p->jengine = false;
+    }
     p->nx_total = xo;
     for (int k = 0; k < NPAIR_CLASSES; ++k)   // kernels queue ket indices in 28 bits
         if (p->pc_off[k + 1] - p->pc_off[k] >= (1 << 28))
@@ -1352,6 +1356,9 @@ extern "C" int jk_plan_set_shard(jk_plan *plan, int rank, int size)
 extern "C" int jk_plan_set_jengine(jk_plan *plan, int on)
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_jengine: plan is NULL");
+    if (on && plan->nx_total == 0 && plan->npairs > 0)
+        return fail(JK_ERR_ARG, "jk_plan_set_jengine: the plan's x-space blocks exceed the J "
+                                "engine's index range");
     plan->jengine = on != 0;
     return JK_OK;
 }

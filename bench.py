@@ -150,7 +150,7 @@ def run_reference(args, rank):
     line = {'impl': 'reference', 'metric': 'jk_builds_per_s', 'value': v,
             'unit': 'builds/s', 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 / v, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
             'config': {'workload': args.workload, 'hermi': 1, 'direct_scf_tol': TOL,
                        'form': 'plain'},
             'cpu_baseline': {'value': v, 'unit': 'builds/s', 'cores': threads,

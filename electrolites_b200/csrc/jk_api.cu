@@ -754,7 +754,10 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     a.grouped = jk_class_table[c].form == 0 && E.cls_nview[c] > 1;
     // the J engine: every class of a J-only build; with K, the team-form
     // classes (J from the x-space contraction, K from the transfers)
-    a.jx = E.jx && (E.jx_jonly || jk_class_table[c].form == 1 || E.jx_reg);
+    // (2: a J-only build, whose register-form kernel has no K path)
+    a.jx = E.jx && (E.jx_jonly || jk_class_table[c].form == 1 || E.jx_reg)
+               ? (E.jx_jonly ? 2 : 1)
+               : 0;
     a.jx_dens = E.jx_dens;
     a.jx_acc = E.jx_acc;
     a.nterm = E.nterm;

@@ -95,10 +95,11 @@ struct ClassArgs {
     int nterm;
     double op_coef[2];
     double op_inv_om2[2];
-    // J engine (J-only single-plan builds): 1 = contract each quartet's
-    // (e0|f0) block with the pairs' x-space densities instead of
-    // transferring it to (ij|kl); pair P's block of n_j x NX(P) doubles
-    // starts at P.xoff * n_j in jx_dens (densities) and jx_acc (J)
+    // J engine (single-plan builds): 0 off; 1 = J from each quartet's
+    // (e0|f0) block contracted with the pairs' x-space densities (K, if any,
+    // from the transfers); 2 = the same in a J-only build.  Pair P's block
+    // of n_j x NX(P) doubles starts at P.xoff * n_j in jx_dens (densities)
+    // and jx_acc (J)
     int jx;
     const double *jx_dens;
     double *jx_acc;

@@ -12,16 +12,23 @@ plain all-FP64 form.  One step = one J/K build of both densities.
                     [--workload NAME] [--mixed THRESHOLD]
 
 Prints one JSON line (rank 0).  value = J/K builds per second of the whole
-job (device-timed with CUDA events, densities resident in HBM); e2e = the
-same through jk_build_host from pinned host buffers, copies included.  With
-N > 1 ranks (torchrun, one GPU each) the build is sharded: every rank
-evaluates the tasks rank, rank + N, ... of each class launch and one NCCL
-all-reduce of the (vj, vk) buffer completes the build on every rank (strong
-scaling: one build per step for the whole job); timing is the max over
-ranks.  The default run also reports the plain-vs-mixed threshold sweep
-(1e-10..1e-6) on this workload and on (H2O)_64 def2-TZVP, the uneven
-512-molecule batch (one build per molecule vs batched FP64 vs batched
-mixed) and a serving run.
+job (device-timed with CUDA events, densities resident in HBM, the default
+launch path: no per-class events); e2e = the same through jk_build_host from
+pinned host buffers, copies included.  A second, separately timed pass with
+per-class events on the class streams (the same launch order) gives the
+dominant class kernel's in-situ time for the roofline.  With N > 1 ranks
+(one GPU each; `--gpus N` starts them itself through torch.distributed.run
+when WORLD_SIZE is unset) the build is sharded: every rank evaluates the
+tasks rank, rank + N, ... of each class launch and one NCCL all-reduce of
+the (vj, vk) buffer completes the build on every rank (strong scaling: one
+build per step for the whole job); timing is the max over ranks.
+
+The default run also reports: the timed build's errors against the fast
+FP64 CPU checker (oracle/jk_check.c), whose full, unsampled build of the
+same workload on all host cores is the CPU baseline; the plain-vs-mixed
+threshold sweep (1e-10..1e-6) on this workload and on (H2O)_64 def2-TZVP,
+each with its errors against the checker; the uneven 512-molecule batch;
+a serving sweep over request rates.
 """
 from __future__ import annotations
 
@@ -32,6 +39,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -111,49 +119,83 @@ class ClockSampler:
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_sample(mol, dms, budget_s=15.0, nthreads=0, seed=1):
-    """Oracle J/K on a random sample of bra shell pairs, scaled to a full
-    build: returns (builds/s, threads, description)."""
-    import numpy as np
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def checker_build(mol, dms, nthreads=0, shard=0, nshard=1):
+    """The fast FP64 CPU checker (oracle/jk_check.c) on `nthreads` host
+    threads: (vj, vk, quartets, seconds) of bra-pair shard `shard` of
+    `nshard` (0 of 1: the whole build)."""
     from oracle import oracle as O
-    nthreads = nthreads or os.cpu_count() or 1
-    npair = mol.nbas * (mol.nbas + 1) // 2
-    rng = np.random.default_rng(seed)
-    n, spent, nq_tot, used = 8, 0.0, 0, 0
-    while spent < budget_s and used < npair:
-        take = rng.choice(npair, size=min(n, npair - used), replace=False)
-        t0 = time.perf_counter()
-        _, _, nq = O.jk_sample(mol, dms, take, tol=TOL, nthreads=nthreads)
-        spent += time.perf_counter() - t0
-        used += len(take)
-        nq_tot += nq
-        n = max(8, int(n * min(4.0, max(1.5, budget_s / max(spent, 1e-3) / 2))))
-    t_full = spent * npair / used
-    desc = (f'{used} of {npair} bra shell pairs drawn uniformly (seed {seed}), all '
-            f'their kets, {nq_tot} quartets in {spent:.1f} s; time scaled by '
-            f'{npair / used:.1f} to a full build')
-    return 1.0 / t_full, nthreads, desc
+    t0 = time.perf_counter()
+    vj, vk, nq = O.jk_fast(mol, dms, tol=TOL, nthreads=nthreads or host_cores(),
+                           shard=shard, nshard=nshard)
+    return vj, vk, nq, time.perf_counter() - t0
+
+
+class BackgroundCheck(threading.Thread):
+    """A checker build on a worker thread (ctypes releases the GIL), so that
+    the host cores work while the GPU runs other measurements."""
+
+    def __init__(self, mol, dms, nthreads):
+        super().__init__(daemon=True)
+        self.args = (mol, dms, nthreads)
+        self.result = None
+        self.error = None
+
+    def run(self):
+        try:
+            self.result = checker_build(*self.args)
+        except Exception as err:   # noqa: BLE001
+            self.error = err
+
+
+def errors_vs(dms, vj, vk, rj, rk):
+    """Largest element errors and energy errors (E_J = 1/2 tr(D J),
+    E_K = -1/4 tr(D K), summed over the densities) of (vj, vk) against the
+    checker's (rj, rk)."""
+    import numpy as np
+    ej = 0.5 * np.einsum('nij,nji->', dms, vj) - 0.5 * np.einsum('nij,nji->', dms, rj)
+    ek = -0.25 * np.einsum('nij,nji->', dms, vk) + 0.25 * np.einsum('nij,nji->', dms, rk)
+    return {'max_dJ': float(np.abs(vj - rj).max()), 'max_dK': float(np.abs(vk - rk).max()),
+            'dE_J': float(ej), 'dE_K': float(ek)}
+
+
+REF_SHARDS = 8
 
 
 def run_reference(args, rank):
+    """The CPU arm: the fast FP64 checker (the restated reference algorithm,
+    oracle/jk_check.c) on all host cores.  Step s builds bra-pair shard
+    s mod 8 of 8 of the workload (interleaved bra pairs, so every shard has
+    the same mix), so 8 consecutive steps are one full, unsampled build and
+    the timed region covers whole builds; value = builds per second."""
     if rank != 0:
         return
     mol, dms = make_inputs(args.workload)
-    vals = []
-    threads, desc = os.cpu_count(), ''
+    cores = host_cores()
+    times = []
     for it in range(args.warmup + args.steps):
-        v, threads, desc = cpu_sample(mol, dms, budget_s=min(20.0, 60.0 / max(1, args.steps)),
-                                      seed=1 + it)
+        _, _, _, dt = checker_build(mol, dms, cores, it % REF_SHARDS, REF_SHARDS)
         if it >= args.warmup:
-            vals.append(v)
-    v = statistics.mean(vals)
+            times.append(dt)
+    step_s = sum(times) / len(times)
+    v = (1.0 / REF_SHARDS) / step_s
+    desc = (f'fast FP64 checker (oracle/jk_check.c), {cores} threads; step = bra-pair shard '
+            f'(s mod {REF_SHARDS}) of {REF_SHARDS} of the full build, so {REF_SHARDS} steps '
+            f'are one unsampled build')
     line = {'impl': 'reference', 'metric': 'jk_builds_per_s', 'value': v,
             'unit': 'builds/s', 'n_gpus': args.gpus, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': 1e3 / v, 'higher_is_better': True,
+            'warmup': args.warmup, 'ms_per_step': step_s * 1e3, 'higher_is_better': True,
             'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': {'workload': args.workload, 'hermi': 1, 'direct_scf_tol': TOL,
-                       'form': 'plain'},
-            'cpu_baseline': {'value': v, 'unit': 'builds/s', 'cores': threads,
+            'config': {'workload': args.workload, 'nao_cart': mol.nao_cart, 'n_dm': int(dms.shape[0]),
+                       'hermi': 1, 'direct_scf_tol': TOL, 'form': 'plain',
+                       'builds_per_step': 1.0 / REF_SHARDS},
+            'cpu_baseline': {'value': v, 'unit': 'builds/s', 'cores': cores,
                              'kind': 'port', 'sample': desc},
             'e2e': {'value': v, 'unit': 'builds/s', 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 0}}
@@ -262,17 +304,18 @@ MIXED_SWEEP = (1e-10, 1e-8, 1e-7, 1e-6)
 MIXED_WORKLOADS = ('h2o96_631gs_uhf', 'h2o64_tzvp')
 
 
-def run_mixed(args, dev, stream, flush):
+def run_mixed(args, dev, stream, flush, workloads=MIXED_WORKLOADS):
     """Plain FP64 against the mixed form at each threshold of the sweep, on
     the (H2O)_96 6-31G* UHF pair and (H2O)_64 def2-TZVP: device ms per build,
     the fraction of quartets run in FP32, and the J/K energy and largest
     element errors against the plain build (E_J = 1/2 tr(D J),
-    E_K = -1/4 tr(D K) summed over the densities)."""
+    E_K = -1/4 tr(D K) summed over the densities).  Returns the table and
+    each form's (vj, vk) on the host, for the errors against the checker."""
     import torch
 
     from electrolites_b200.jk import VHFOpt
-    out = {}
-    for w in MIXED_WORKLOADS:
+    out, host = {}, {}
+    for w in workloads:
         mol, dms_h = make_inputs(w)
         opt = VHFOpt(mol, TOL, device=dev.index).build()
         dms = torch.as_tensor(dms_h, device=dev)
@@ -301,7 +344,22 @@ def run_mixed(args, dev, stream, flush):
                 'max_dJ': float((m[4] - p[4]).abs().max()),
                 'max_dK': float((m[5] - p[5]).abs().max())}
         out[w] = row
-    return out
+        host[w] = (mol, dms_h, {thr: (r[4].cpu().numpy(), r[5].cpu().numpy())
+                                for thr, r in res.items()})
+        del opt, res
+    return out, host
+
+
+def mixed_vs_checker(table, host, checks):
+    """Adds each form's errors against the checker: 'vs_checker' per row
+    (plain) and per threshold."""
+    for w, (mol, dms_h, arrs) in host.items():
+        if w not in checks:
+            continue
+        rj, rk = checks[w]
+        table[w]['plain_vs_checker'] = errors_vs(dms_h, *arrs[0.0], rj, rk)
+        for thr in MIXED_SWEEP:
+            table[w]['thresholds'][f'{thr:g}']['vs_checker'] = errors_vs(dms_h, *arrs[thr], rj, rk)
 
 
 RSH_OMEGA, RSH_LR, RSH_SR = 0.3, 1.0, 0.157706   # an omega-B97X-type exchange mixture
@@ -390,31 +448,54 @@ def run_scf_screen(args, dev, stream, opt, dms_h):
             'speedup': round(tight['ms'] / lt['ms'], 3)}
 
 
+SERVE_FORMS = {'plain': (0.0, False), 'mixed': (BATCH_MIXED, False),
+               'mixed_incremental': (BATCH_MIXED, True)}
+
+
 def run_serve(args, dev):
     """Serving: Poisson arrivals of water-cluster requests (3-60 waters,
     6-31G* or def2-SVP, 1-4 densities, 10 SCF-like cycles with a 1e-4
     relative density perturbation per cycle), continuous batching over
-    resident plans with admission by an HBM budget (half the device).
-    Plain and mixed forms at each rate, and the mixed form with incremental
-    builds (cycles between full rebuilds every 5th build J/K of the density
-    change); mols/s and latency percentiles."""
+    resident plans with admission by an HBM budget (half the device).  For
+    each rate and form: mols/s, latency percentiles, the run's length and
+    whether p99 stayed bounded (below half the run length: requests did not
+    pile up); the highest bounded rate per form.  Rates below the server's
+    capacity (about 1.5 requests/s of this workload on one GPU) take
+    --serve-low-requests requests, the others --serve-requests."""
     from electrolites_b200.serve import JKServer, latency_stats, poisson_requests
-    out = {'workload': 'serve_h2o3-60_631gs_svp', 'requests': args.serve_requests,
-           'cycles': 10, 'hbm_budget': 'half of device memory', 'rates': []}
+    out = {'workload': 'serve_h2o3-60_631gs_svp', 'cycles': 10,
+           'hbm_budget': 'half of device memory', 'forms': list(args.serve_forms), 'rates': []}
+    best = {f: None for f in args.serve_forms}
     for rate in args.serve_rates:
-        row = {'rate_req_per_s': rate}
-        for form, thr, inc in (('plain', 0.0, False), ('mixed', BATCH_MIXED, False),
-                               ('mixed_incremental', BATCH_MIXED, True)):
-            reqs = poisson_requests(args.serve_requests, rate, SERVE_SEED)
+        n_req = args.serve_low_requests if rate <= 2.0 else args.serve_requests
+        row = {'rate_req_per_s': rate, 'requests': n_req}
+        for form in args.serve_forms:
+            thr, inc = SERVE_FORMS[form]
+            reqs = poisson_requests(n_req, rate, SERVE_SEED)
             srv = JKServer(dev.index, hbm_budget=0.5, mixed_threshold=thr, incremental=inc,
                            rebuild_every=5)
             srv.run(reqs)
             st = latency_stats(reqs)
-            row[form] = {k: round(v, 3) for k, v in st.items()}
-            row[form]['mean_batch'] = round(sum(srv.batch_sizes) / len(srv.batch_sizes), 2)
-            row[form]['iterations'] = srv.iterations
+            span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+            r = {k: round(v, 3) for k, v in st.items()}
+            r['run_s'] = round(span, 2)
+            r['p99_bounded'] = bool(st['p99_ms'] * 1e-3 < 0.5 * span)
+            r['mean_batch'] = round(sum(srv.batch_sizes) / len(srv.batch_sizes), 2)
+            r['iterations'] = srv.iterations
+            row[form] = r
+            if r['p99_bounded'] and (best[form] is None or rate > best[form]):
+                best[form] = rate
         out['rates'].append(row)
+    out['highest_bounded_rate'] = best
     return out
+
+
+# DRAM traffic of the dominant class kernel per screened quartet, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of its launch on the
+# (H2O)_32 6-31G* UHF case, scaled to the bench build by its quartet count
+# (the kernel streams pair data and densities in proportion to the quartets
+# it evaluates).  Source: profiles/jk_reg_kernel_ps_ss_h2o32_631gs_uhf_full.md.
+TRAFFIC_PER_QUARTET = {(1, 0, 0, 0): None}
 
 
 def run_ours(args, rank, world):
@@ -433,7 +514,6 @@ def run_ours(args, rank, world):
     mol, dms_h = make_inputs(args.workload)
     n_dm = dms_h.shape[0]
     opt = VHFOpt(mol, TOL, device=local).build()
-    opt.set_timing(True)
     dms = torch.as_tensor(dms_h, device=dev)
     # vj and vk in one buffer: with N > 1 ranks each rank builds its share of
     # every class's tasks and one all-reduce of the buffer completes J and K
@@ -458,36 +538,48 @@ def run_ours(args, rank, world):
     _lib.check(_lib.lib().jk_fp64_peak(local, ctypes.byref(peak)), 'jk_fp64_peak')
     peak_tflops = peak.value
 
+    def timed_steps(per_class):
+        """K device-timed builds (L2 flushed, untimed, before each); with
+        per_class, also the class kernels' in-situ times summed."""
+        evs, class_ms = [], {}
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()                               # L2 flush, outside the timing
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            one()
+            e.record(stream)
+            evs.append((s, e))
+            if per_class:
+                cm, _ = opt.last_class_ms()              # syncs; between steps
+                for k, v in cm.items():
+                    class_ms[k] = class_ms.get(k, 0.0) + v
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        total = sum(s.elapsed_time(e) for s, e in evs)
+        if world > 1:
+            t = torch.tensor([total], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total / args.steps, {k: v / args.steps for k, v in class_ms.items()}
+
+    # the headline: the default launch path, no per-class events
     clocks = ClockSampler(local)
     clocks.start()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    evs = []
-    class_ms = {}
-    launches = 0
-    for _ in range(args.steps):
-        flush.zero_()                                   # L2 flush, outside the timing
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        one()
-        e.record(stream)
-        evs.append((s, e))
-        cm, launches = opt.last_class_ms()             # syncs; between steps
-        for k, v in cm.items():
-            class_ms[k] = class_ms.get(k, 0.0) + v
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    ms_per_step, _ = timed_steps(False)
     clk = clocks.stop()
     opt.sync(stream)
-    step_ms = [s.elapsed_time(e) for s, e in evs]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
+    _, launches = opt.last_class_ms()
+    vj_timed, vk_timed = vj.cpu().numpy(), vk.cpu().numpy()
+
+    # the class kernels' in-situ times: the same launch order (two class
+    # streams) with each class's events on its own stream, timed separately
+    opt.set_timing(2)
+    ms_instrumented, class_ms = timed_steps(True)
+    opt.set_timing(False)
 
     # algorithmic flops of one build
     stats = opt.class_counts()         # this rank's share when sharded
@@ -498,11 +590,11 @@ def run_ours(args, rank, world):
         t = torch.tensor([float(flops), float(nq)], dtype=torch.float64, device=dev)
         dist.all_reduce(t)
         flops, nq = float(t[0]), int(t[1])
-    for k in class_ms:
-        class_ms[k] /= args.steps
     dom = max(class_ms, key=class_ms.get) if class_ms else None
     dom_flops = flop_model.build_flops({dom: stats[dom]}, n_j, n_k) if dom else 0
     achieved = dom_flops / (class_ms[dom] * 1e-3) / 1e12 if dom else 0.0
+    tpq = TRAFFIC_PER_QUARTET.get(dom)
+    traffic = tpq * stats[dom][0] if (dom and tpq) else None
 
     # e2e through the host-buffer entry point, pinned buffers
     dm_pin = torch.as_tensor(dms_h).pin_memory()
@@ -539,35 +631,55 @@ def run_ours(args, rank, world):
         e2e_s = float(t.item())
     bytes_in = dm_pin.numel() * 8
     bytes_out = 2 * dm_pin.numel() * 8
+    assert np.isfinite(vj_timed).all() and np.isfinite(vk_timed).all()
 
-    # correctness guard on the timed output: symmetric, finite
-    assert torch.isfinite(vj).all() and torch.isfinite(vk).all()
+    solo = rank == 0 and world == 1
+    check = solo and not args.no_check
+    # the def2-TZVP checker build runs on the host cores while the GPU
+    # measures the other forms (it is not a timed CPU number)
+    bg = None
+    if check and not args.no_mixed and 'h2o64_tzvp' in MIXED_WORKLOADS:
+        mol2, dms2 = make_inputs('h2o64_tzvp')
+        bg = BackgroundCheck(mol2, dms2, max(1, host_cores() - 2))
+        bg.start()
 
-    rsh = None
-    if rank == 0 and world == 1 and not args.no_rsh:
-        rsh = run_rsh(args, dev, stream, flush, opt, dms)
-
-    scf_screen = None
-    if rank == 0 and world == 1 and not args.no_scf_screen:
-        scf_screen = run_scf_screen(args, dev, stream, opt, dms_h)
-
-    mixed = None
-    if rank == 0 and world == 1 and not args.no_mixed:
-        mixed = run_mixed(args, dev, stream, flush)
-
+    rsh = run_rsh(args, dev, stream, flush, opt, dms) if solo and not args.no_rsh else None
+    scf_screen = (run_scf_screen(args, dev, stream, opt, dms_h)
+                  if solo and not args.no_scf_screen else None)
+    mixed = mixed_host = None
+    if solo and not args.no_mixed:
+        mixed, mixed_host = run_mixed(args, dev, stream, flush)
     batched = None
-    if rank == 0 and world == 1 and not args.no_batch:
+    if solo and not args.no_batch:
         batched = run_batch(args, dev, stream, flush, peak_tflops)
-
     serving = None
-    if rank == 0 and world == 1 and args.serve_requests > 0:
+    if solo and args.serve_forms and args.serve_rates:
         serving = run_serve(args, dev)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, thr_used, desc = cpu_sample(mol, dms_h, budget_s=args.cpu_budget)
-        cpu = {'value': v, 'unit': 'builds/s', 'cores': thr_used, 'kind': 'port',
-               'sample': desc}
+    # CPU baseline: one full, unsampled checker build of the workload on all
+    # host cores (nothing else running), which is also the parity reference
+    # of the timed GPU build
+    cpu = parity = None
+    if bg is not None:
+        bg.join()
+    if check:
+        cores = host_cores()
+        rj, rk, cnq, cs = checker_build(mol, dms_h, cores)
+        cpu = {'value': 1.0 / cs, 'unit': 'builds/s', 'cores': cores, 'kind': 'port',
+               'sample': f'one full, unsampled build of {args.workload} ({cnq} quartets) by the '
+                         f'fast FP64 checker oracle/jk_check.c in {cs:.1f} s'}
+        parity = errors_vs(dms_h, vj_timed, vk_timed, rj, rk)
+        parity.update({'checker': 'oracle/jk_check.c', 'element_tol': 1e-10,
+                       'energy_tol_eh': 1e-9,
+                       'pass': parity['max_dJ'] <= 1e-10 and parity['max_dK'] <= 1e-10 and
+                       abs(parity['dE_J']) <= 1e-9 and abs(parity['dE_K']) <= 1e-9})
+        checks = {args.workload: (rj, rk)}
+        if bg is not None and bg.result is not None:
+            checks['h2o64_tzvp'] = bg.result[:2]
+        if mixed is not None:
+            mixed_vs_checker(mixed, mixed_host, checks)
+        if bg is not None and bg.error is not None:
+            parity['tzvp_check_error'] = str(bg.error)
 
     if rank == 0:
         line = {
@@ -582,20 +694,26 @@ def run_ours(args, rank, world):
                        'parallelism': 'one GPU' if world == 1 else
                        f'{world} ranks, tasks interleaved, one NCCL all-reduce of vj/vk',
                        'l2': 'flushed between steps (256 MB write, untimed)',
+                       'timed_path': 'default launch order (two class streams, no per-class events)',
                        'quartets': nq, 'build_tflops': flops / (ms_per_step * 1e-3) / 1e12,
                        'fp64_peak_tflops': peak_tflops,
                        'fp64_peak_frac': flops / (ms_per_step * 1e-3) / 1e12 / peak_tflops,
+                       'instrumented_ms_per_step': ms_instrumented,
                        'class_ms': {''.join(map(str, k)): round(v, 3) for k, v in
                                     sorted(class_ms.items(), key=lambda kv: -kv[1])[:12]}},
             'roofline': {'bound': 'fp64', 'kernel': 'jk_class_kernel ' + ''.join(map(str, dom)) if dom else None,
                          'achieved': achieved, 'peak': peak_tflops, 'unit': 'TFLOP/s',
                          'frac': achieved / peak_tflops if peak_tflops else None,
                          'peak_source': 'in-run FP64 FMA probe (jk_fp64_peak)',
-                         'traffic': None},
+                         'duration_source': 'class events on the class streams, separate timed pass',
+                         'traffic': traffic,
+                         'traffic_source': 'ncu dram bytes per quartet of this kernel on (H2O)_32, '
+                                           'scaled by the quartet count' if traffic else None},
             'e2e': {'value': 1.0 / e2e_s, 'unit': 'builds/s', 'h2d_bytes_per_step': bytes_in,
                     'd2h_bytes_per_step': bytes_out},
             'gpu_launches': launches * args.steps,
             'clocks': clk,
+            'parity': parity,
             'cpu_baseline': cpu,
             'mixed': mixed,
             'range_separated': rsh,
@@ -606,6 +724,54 @@ def run_ours(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_dry(args, rank, world):
+    """The multi-rank launcher and exchange without a GPU (gloo): each rank
+    adds a rank-dependent share of a fixed matrix, one all-reduce sums the
+    shares, rank 0 checks the sum and prints the JSON line shape.  It times
+    nothing and claims no throughput."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    full = np.arange(64, dtype=np.float64).reshape(8, 8)
+    share = np.where(np.arange(64).reshape(8, 8) % world == rank, full, 0.0)
+    buf = torch.as_tensor(share)
+    if world > 1:
+        dist.all_reduce(buf)
+    ok = bool(np.array_equal(buf.numpy(), full))
+    if rank == 0:
+        print(json.dumps({'metric': 'jk_builds_per_s', 'value': None, 'unit': 'builds/s',
+                          'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+                          'dry_run': True, 'exchange_ok': ok,
+                          'config': {'workload': args.workload, 'parallelism':
+                                     f'{world} ranks (gloo, no GPU)'}}), flush=True)
+    if not ok:
+        raise SystemExit('dry run: the all-reduced shares do not sum to the matrix')
+
+
+def launch_ranks(args):
+    """`--gpus N` without a launcher: start N ranks through
+    torch.distributed.run on this node (127.0.0.1) and return their exit
+    code.  Fails when fewer than N CUDA devices are visible."""
+    import socket
+    if not args.dry_run:
+        import torch
+        n = torch.cuda.device_count()
+        if n < args.gpus:
+            raise SystemExit(f'bench.py: --gpus {args.gpus} but {n} CUDA device(s) visible')
+    with socket.socket() as sk:
+        sk.bind(('127.0.0.1', 0))
+        port = sk.getsockname()[1]
+    env = dict(os.environ)
+    if not args.dry_run:
+        # NCCL's communicator set-up lines name the rank count
+        env.setdefault('NCCL_DEBUG', 'INFO')
+        env.setdefault('NCCL_DEBUG_SUBSYS', 'INIT')
+    cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1',
+           f'--nproc-per-node={args.gpus}', '--master-addr=127.0.0.1',
+           f'--master-port={port}', os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd, env=env)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -614,12 +780,16 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument('--mixed', type=float, default=0.0)
-    ap.add_argument('--cpu-budget', type=float, default=15.0)
-    ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--serve-requests', type=int, default=32,
-                    help='requests per serving run (0: skip serving)')
-    ap.add_argument('--serve-rates', type=float, nargs='+', default=[50.0],
+    ap.add_argument('--no-check', action='store_true',
+                    help='skip the checker builds (parity, CPU baseline, mixed errors)')
+    ap.add_argument('--serve-rates', type=float, nargs='*', default=[0.5, 1.0, 2.0, 50.0, 2000.0],
                     help='Poisson arrival rates (requests/s) of the serving runs')
+    ap.add_argument('--serve-requests', type=int, default=24,
+                    help='requests per serving run above 2 requests/s')
+    ap.add_argument('--serve-low-requests', type=int, default=12,
+                    help='requests per serving run at 2 requests/s or less')
+    ap.add_argument('--serve-forms', nargs='*', default=['plain', 'mixed_incremental'],
+                    choices=sorted(SERVE_FORMS), help='server forms to run (none: skip serving)')
     ap.add_argument('--no-mixed', action='store_true',
                     help='skip the plain-vs-mixed threshold sweep')
     ap.add_argument('--no-scf-screen', action='store_true',
@@ -628,21 +798,32 @@ def main():
                     help='skip the fused range-separated exchange comparison')
     ap.add_argument('--no-batch', action='store_true',
                     help='skip the uneven-batch comparison (plain vs batched vs mixed)')
+    ap.add_argument('--dry-run', action='store_true',
+                    help='launcher and exchange only, on CPU ranks (gloo); no GPU, no timing')
     args = ap.parse_args()
+    if args.gpus > 1 and 'WORLD_SIZE' not in os.environ and args.impl == 'ours':
+        sys.exit(launch_ranks(args))
     world = int(os.environ.get('WORLD_SIZE', 1))
     rank = int(os.environ.get('RANK', 0))
     if args.impl == 'reference':
         run_reference(args, rank)
         return
+    if 'WORLD_SIZE' in os.environ and world != args.gpus:
+        raise SystemExit(f'bench.py: --gpus {args.gpus} but WORLD_SIZE={world}')
     if world > 1:
         import datetime
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+        if not args.dry_run:
+            torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        dist.init_process_group('gloo' if args.dry_run else 'nccl',
+                                timeout=datetime.timedelta(seconds=600))
     try:
-        run_ours(args, rank, world)
+        if args.dry_run:
+            run_dry(args, rank, world)
+        else:
+            run_ours(args, rank, world)
     finally:
         if world > 1:
             import torch.distributed as dist

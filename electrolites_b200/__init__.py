@@ -73,17 +73,34 @@ def _out(x, like):
     return x
 
 
+def _resolve_omega(opt, omega):
+    """The operator's omega: the caller's, else the one riding on the option
+    object's molecule, as the reference resolves it (resolve_rsh,
+    electrolites/compat.py:178-187, called at electrolites/fastjk.py:287 and
+    electrolites/fastk.py:661): GPU4PySCF sets the range of a
+    range-separated functional on that mol.  None when neither names one."""
+    if omega is not None:
+        return omega
+    for name in ('mol', 'sorted_mol'):
+        m = getattr(opt, name, None)
+        w = getattr(m, 'omega', None) if m is not None else None
+        if w:
+            return float(w)
+    return None
+
+
 def _get_jk(self, dms, hermi, verbose=None):
     if callable(dms):
         dms = dms()
-    vj, vk = _plan_for(self).get_jk(dms, hermi, verbose)
+    vj, vk = _plan_for(self).get_jk(dms, hermi, verbose, omega=_resolve_omega(self, None))
     return _out(vj, dms), _out(vk, dms)
 
 
 def _get_k(self, dms, hermi, verbose=None, omega=None, lr_factor=None, sr_factor=None):
     if callable(dms):
         dms = dms()
-    return _out(_plan_for(self).get_k(dms, hermi, verbose, omega, lr_factor, sr_factor), dms)
+    return _out(_plan_for(self).get_k(dms, hermi, verbose, _resolve_omega(self, omega),
+                                      lr_factor, sr_factor), dms)
 
 
 def _get_j(self, dms, verbose=None):

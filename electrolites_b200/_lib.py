@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, 'libjk_b200.so')
 
 JK_ERRORS = {1: 'invalid argument', 2: 'unsupported shell', 3: 'CUDA error',
              4: 'out of device memory', 5: 'density out of the plan range',
-             6: 'kernel error flag'}
+             6: 'kernel error flag', 7: 'beyond the allocation-free scratch'}
 
 EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_build_host', 'jk_sync', 'jk_last_counts', 'jk_class_info',

@@ -181,6 +181,7 @@ struct Engine {
     double *jx_Jh = nullptr;
     int jx_nj = 0;
     bool timing = false;
+    int timing_mode = 0;            // 1: serialised on one stream, 2: on the class streams
     std::vector<cudaEvent_t> ev;    // 2 per class
     std::vector<char> ev_used;
     int launches = 0;
@@ -318,7 +319,7 @@ static int engine_idle(Engine &E)
 static int engine_reserve_rows(Engine &E, long long rows, bool no_alloc, const char *who)
 {
     if (rows <= E.max_rows) return JK_OK;
-    if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": task rows beyond the plan's reservation");
+    if (no_alloc) return fail(JK_ERR_SCRATCH, std::string(who) + ": task rows beyond the plan's reservation");
     RC(engine_idle(E));
     cudaFree(E.d_rows);
     cudaFree(E.d_cub);
@@ -343,7 +344,7 @@ static int engine_reserve_rows(Engine &E, long long rows, bool no_alloc, const c
 static int engine_reserve_blob(Engine &E, size_t bytes, bool no_alloc, const char *who)
 {
     if (bytes <= E.blob_cap) return JK_OK;
-    if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": descriptors beyond the plan's reservation");
+    if (no_alloc) return fail(JK_ERR_SCRATCH, std::string(who) + ": descriptors beyond the plan's reservation");
     RC(engine_idle(E));
     cudaFree(E.d_blob);
     if (E.h_blob) cudaFreeHost(E.h_blob);
@@ -472,14 +473,14 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     char *ws = nullptr;
     if (ws_ext) {
         if (need > ws_ext_size)
-            return fail(JK_ERR_RANGE, std::string(who) + ": this build needs " + std::to_string(need) +
+            return fail(JK_ERR_SCRATCH, std::string(who) + ": this build needs " + std::to_string(need) +
                                           " bytes of scratch, the library's static scratch holds " +
                                           std::to_string(ws_ext_size) +
                                           " (use jk_build for larger molecules or more densities)");
         ws = ws_ext;
     } else {
         if (need > E.ws_size) {
-            if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": workspace beyond reservation");
+            if (no_alloc) return fail(JK_ERR_SCRATCH, std::string(who) + ": workspace beyond reservation");
             RC(engine_idle(E));
             cudaFree(E.d_ws);
             E.d_ws = nullptr;
@@ -604,7 +605,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     }
     E.ncounters = ncounters;
     if (ncounters > E.counter_cap) {
-        if (no_alloc) return fail(JK_ERR_ARG, std::string(who) + ": counters beyond reservation");
+        if (no_alloc) return fail(JK_ERR_SCRATCH, std::string(who) + ": counters beyond reservation");
         RC(engine_idle(E));
         cudaFree(E.d_counters);
         E.d_counters = nullptr;
@@ -863,9 +864,10 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
     cfg.configure_only = 0;
     cfg.msg = msg;
     // fork the class streams off the build's stream (also inside a capture);
-    // with per-class timing on, one stream, so that each class's events
-    // bracket its own kernels only
-    const int ns = timing ? 1 : JK_CLASS_STREAMS;
+    // with serialised per-class timing (mode 1) one stream, so that each
+    // class's events bracket its own kernels only; mode 2 keeps the class
+    // streams and records each class's events on its own stream
+    const int ns = timing && E.timing_mode == 1 ? 1 : JK_CLASS_STREAMS;
     cudaStream_t cs[JK_CLASS_STREAMS];
     cs[0] = st;
     if (ns > 1) CK(cudaEventRecord(E.ev_fork, st));
@@ -994,7 +996,9 @@ static int engine_set_timing(Engine &E, int enable)
         for (auto &e : E.ev) CK(cudaEventCreate(&e));
         E.ev_used.assign(JK_NCLASSES, 0);
     }
+    if (enable < 0 || enable > 2) return fail(JK_ERR_ARG, "timing mode must be 0, 1 or 2");
     E.timing = enable != 0;
+    E.timing_mode = enable;
     return JK_OK;
 }
 

@@ -32,7 +32,9 @@ molecule's own AO basis (spherical unless ``mol.cart``) and transform them.
 """
 from __future__ import annotations
 
+import collections
 import ctypes
+import hashlib
 
 import numpy as np
 
@@ -238,7 +240,11 @@ class VHFOpt:
         return out
 
     def set_timing(self, enable=True):
-        _lib.check(_lib.lib().jk_set_timing(self.plan, int(bool(enable))), 'jk_set_timing')
+        """Per-class kernel events: True / 1 times each class alone (class
+        kernels serialised on the build's stream), 2 records the events on
+        the class streams of the default launch order, False / 0 none."""
+        mode = 2 if enable == 2 else int(bool(enable))
+        _lib.check(_lib.lib().jk_set_timing(self.plan, mode), 'jk_set_timing')
 
     def last_class_ms(self):
         """({(li, lj, lk, ll): ms of that class kernel in the last build},
@@ -328,17 +334,36 @@ def _rsh_terms(omega, lr_factor, sr_factor):
 # ----------------------------------------------------------------------
 # module-level functions (GPU4PySCF's jk.get_jk / get_j / get_k)
 # ----------------------------------------------------------------------
-_OPTS = {}
+# plans of the module functions, keyed by the molecule's content (geometry,
+# basis, AO layout and screening threshold), least recently used last out:
+# a molecule moved in place (PySCF's set_geom_ defaults to inplace=True, as
+# do scanners) gets a new plan, and the cache holds at most _OPTS_MAX plans
+_OPTS = collections.OrderedDict()
+_OPTS_MAX = 8
+
+
+def _opt_key(mol):
+    h = hashlib.sha1()
+    for a, dt in ((mol._atm, np.int32), (mol._bas, np.int32), (mol._env, np.float64)):
+        h.update(np.ascontiguousarray(a, dtype=dt).tobytes())
+        h.update(b'|')
+    h.update(np.ascontiguousarray(mol.ao_loc_nr(cart=True), dtype=np.int64).tobytes())
+    tol = float(getattr(mol, 'direct_scf_tol', DEFAULT_TOL))
+    return h.hexdigest(), tol
 
 
 def _opt_for(mol, vhfopt):
     if vhfopt is not None:
         return vhfopt
-    key = id(mol)
+    key = _opt_key(mol)
     opt = _OPTS.get(key)
-    if opt is None or opt.mol is not mol:
-        opt = VHFOpt(mol, getattr(mol, 'direct_scf_tol', DEFAULT_TOL)).build()
+    if opt is None:
+        opt = VHFOpt(mol, key[1]).build()
         _OPTS[key] = opt
+        while len(_OPTS) > _OPTS_MAX:
+            _OPTS.popitem(last=False)
+    else:
+        _OPTS.move_to_end(key)
     return opt
 
 

@@ -39,6 +39,9 @@ extern "C" {
 #define JK_ERR_NOMEM 4        /* device allocation failed                  */
 #define JK_ERR_RANGE 5        /* density beyond the plan's screening range */
 #define JK_ERR_DEVICE 6       /* error flag raised inside a kernel         */
+#define JK_ERR_SCRATCH 7      /* jk_build_noalloc: the build needs more scratch
+                                 than the library's fixed array (or the plan's
+                                 reservation) holds; jk_build can run it     */
 
 typedef struct jk_plan jk_plan;
 
@@ -132,8 +135,10 @@ int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi,
  * the library keeps until the process exits.  A build whose scratch would
  * not fit -- about n_k + 2 n_j density-sized double matrices plus
  * nbas^2 floats, e.g. nao up to ~700 for two symmetric densities -- is
- * rejected with JK_ERR_RANGE before anything is launched.  The plan must
- * already exist (jk_plan_create allocates; create it at set-up).
+ * rejected with JK_ERR_SCRATCH before anything is launched.  The plan must
+ * already exist (jk_plan_create allocates; create it at set-up); its
+ * create-time reservations cover its own builds, so jk_build_noalloc may be
+ * a plan's first build.
  *
  * The first call on a device looks up the array's device address (with
  * that device current); make that first call before any stream capture.
@@ -167,10 +172,13 @@ int jk_last_counts(jk_plan *plan, unsigned long long *quartets,
 int jk_class_info(int k, int *li, int *lj, int *lk, int *ll, int *form);
 
 /*
- * Per-class kernel timing.  With enable = 1 every later build records CUDA
+ * Per-class kernel timing.  enable = 1: every later build records CUDA
  * events around each class kernel and runs all class kernels on the build's
  * stream (otherwise they are spread over two streams to overlap their
- * tails);
+ * tails), so each class is timed alone; enable = 2: the class kernels keep
+ * their two streams and each class's events are recorded on its own stream
+ * (the class times of the default launch order, overlap included);
+ * enable = 0: no events.
  * jk_last_class_ms() then returns the milliseconds of each class kernel of
  * the last build (0 for classes not launched) and the number of kernels the
  * library launched in that build.  Synchronises the last build's stream.

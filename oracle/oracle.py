@@ -131,3 +131,79 @@ def jk_sample(mol, dms, ij_list, tol=1e-13, with_j=True, with_k=True, nthreads=0
     if err:
         raise RuntimeError(f'oracle_jk_sample failed ({err})')
     return vj, vk, nq.value
+
+
+# ---------------------------------------------------------------------------
+# fast FP64 checker (jk_check.c): same arithmetic, double-precision roots from
+# Chebyshev fits of the long-double solver, OpenMP over bra pairs
+# ---------------------------------------------------------------------------
+def _check_lib():
+    L = lib()
+    if not getattr(L, '_check_ready', False):
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.check_rys.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
+        L.check_jk.argtypes = [ip, ip, ctypes.c_int, dp, ip, dp, ctypes.c_int,
+                               ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp,
+                               ctypes.c_int, ctypes.POINTER(ctypes.c_longlong),
+                               ctypes.c_double, ctypes.c_int, ctypes.c_int, dp]
+        L.check_eri_shells.argtypes = [ip, ip, ctypes.c_int, dp, ip, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, dp]
+        L._check_ready = True
+    return L
+
+
+def check_rys(n: int, x: float):
+    r = np.zeros(n)
+    w = np.zeros(n)
+    if _check_lib().check_rys(n, float(x), _p(r), _p(w)):
+        raise ValueError('bad Rys order or argument')
+    return r, w
+
+
+def check_eri_shells(mol, i, j, k, l, omega=0.0):
+    """(ij|kl) of four shells (i >= j, k >= l) through the fast checker."""
+    from electrolites_b200.gto import ncart
+    atm, bas, env = _arrays(mol)
+    ao_loc = np.ascontiguousarray(mol.ao_loc_nr(cart=True), dtype=np.int32)
+    ls = [int(mol._bas[s, 1]) for s in (i, j, k, l)]
+    out = np.zeros([ncart(x) for x in ls])
+    if _check_lib().check_eri_shells(_p(atm, ctypes.c_int), _p(bas, ctypes.c_int), mol.nbas,
+                                     _p(env), _p(ao_loc, ctypes.c_int), i, j, k, l,
+                                     float(omega), _p(out)):
+        raise ValueError('unsupported shell quartet')
+    return out
+
+
+def jk_fast(mol, dms, tol=1e-13, with_j=True, with_k=True, nthreads=0, omega=0.0,
+            shard=0, nshard=1, want_q=False):
+    """(vj, vk, n_quartets[, q_cond]) from the fast FP64 checker: the same
+    quartets and contractions as jk(), restricted to bra shell pairs of shard
+    `shard` of `nshard` (the shards sum to the full build)."""
+    atm, bas, env = _arrays(mol)
+    dms = np.ascontiguousarray(dms, dtype=np.float64)
+    squeeze = dms.ndim == 2
+    if squeeze:
+        dms = dms[None]
+    ao_loc = np.ascontiguousarray(mol.ao_loc_nr(cart=True), dtype=np.int32)
+    vj = np.zeros_like(dms) if with_j else None
+    vk = np.zeros_like(dms) if with_k else None
+    q = np.zeros((mol.nbas, mol.nbas)) if want_q else None
+    nq = ctypes.c_longlong(0)
+    null = ctypes.POINTER(ctypes.c_double)()
+    err = _check_lib().check_jk(
+        _p(atm, ctypes.c_int), _p(bas, ctypes.c_int), mol.nbas, _p(env),
+        _p(ao_loc, ctypes.c_int), _p(dms), dms.shape[0], float(tol), int(with_j),
+        int(with_k), _p(vj) if with_j else null, _p(vk) if with_k else null,
+        int(nthreads), ctypes.byref(nq), float(omega), int(shard), int(nshard),
+        _p(q) if want_q else null)
+    if err:
+        raise RuntimeError(f'check_jk failed ({err})')
+    if vj is None:
+        vj = np.zeros_like(dms)
+    if vk is None:
+        vk = np.zeros_like(dms)
+    if squeeze:
+        vj, vk = vj[0], vk[0]
+    return (vj, vk, nq.value, q) if want_q else (vj, vk, nq.value)

@@ -363,3 +363,42 @@ def test_general_contractions(torch, oracle):
     vj, vk = VHFOpt(gc, TOL).build().get_jk(torch.as_tensor(dms), 0)
     assert np.abs(vj.cpu().numpy() - rj).max() <= ATOL
     assert np.abs(vk.cpu().numpy() - rk).max() <= ATOL
+
+
+# ---------------------------------------------------------------------------
+# Parity at the sizes the benchmark times, against the fast FP64 checker
+# (oracle/jk_check.c, itself checked against the long-double oracle to 1e-12
+# in tests/test_check.py)
+# ---------------------------------------------------------------------------
+BENCH_SHAPES = {
+    # (waters, cube edge A, basis, UHF pair, seed): the bench's workloads
+    'h2o32_631gs_uhf': (32, 10.4, '6-31g*', True, 20261204),
+    'h2o8_tzvp': (8, 6.5, 'def2-tzvp', False, 20261205),
+    'h2o96_631gs_uhf': (96, 15.0, '6-31g*', True, 20261204),
+}
+
+
+def _bench_inputs(name):
+    n, edge, basis, uhf, seed = BENCH_SHAPES[name]
+    mol = clusters.water_mole(n, edge, seed, basis=basis, cart=True)
+    D = clusters.atomic_density(mol, seed)
+    dms = clusters.uhf_pair(D, seed + 1) if uhf else D[None]
+    return mol, np.ascontiguousarray(dms)
+
+
+@pytest.mark.parametrize('name', list(BENCH_SHAPES))
+def test_parity_at_bench_sizes(torch, oracle, name):
+    """Plain FP64 J/K of the benchmark's shapes -- (H2O)_32 6-31G* UHF,
+    (H2O)_8 def2-TZVP, and the headline (H2O)_96 6-31G* UHF build itself --
+    within 1e-10 of the checker on every element and 1e-9 Eh on E_J, E_K."""
+    from electrolites_b200.jk import VHFOpt
+    mol, dms = _bench_inputs(name)
+    opt = VHFOpt(mol, TOL).build()
+    vj, vk = opt.get_jk(torch.as_tensor(dms, device='cuda'), 1)
+    gj, gk = vj.cpu().numpy(), vk.cpu().numpy()
+    rj, rk, _ = oracle.jk_fast(mol, dms, tol=TOL)
+    assert np.abs(gj - rj).max() <= ATOL, np.abs(gj - rj).max()
+    assert np.abs(gk - rk).max() <= ATOL, np.abs(gk - rk).max()
+    ej, ek = _energies(dms, gj, gk)
+    rej, rek = _energies(dms, rj, rk)
+    assert abs(ej - rej) <= ETOL and abs(ek - rek) <= ETOL, (ej - rej, ek - rek)

@@ -144,3 +144,53 @@ def test_flop_model_counts():
     f = F.quartet_flops(0, 0, 0, 0, 1, 1, n_j=1, n_k=1)
     assert f == F.F_PRIM_BASE + 1 * (F.F_ROOT + 3 * F.f_2d(0, 0, 0, 0) + 3 * 1) + 1 * 1 * 2 * 6
     assert F.quartet_flops(2, 2, 2, 2, 1, 1, 1, 1) > F.quartet_flops(1, 1, 1, 1, 1, 1, 1, 1)
+
+
+def test_patched_methods_take_omega_from_the_option_mol(monkeypatch):
+    """After patching, a range-separated functional's omega set on the option
+    object's mol reaches the engine when the call names none (the reference
+    resolves it there, electrolites/compat.py:178-187); an explicit omega
+    wins."""
+    import electrolites_b200 as eb
+    seen = []
+
+    class Plan:
+        def get_jk(self, dms, hermi, verbose=None, omega=None):
+            seen.append(('jk', omega))
+            return dms, dms
+
+        def get_k(self, dms, hermi, verbose=None, omega=None, lr_factor=None, sr_factor=None):
+            seen.append(('k', omega, lr_factor, sr_factor))
+            return dms
+
+    class Opt:
+        pass
+
+    opt = Opt()
+    opt.mol = types.SimpleNamespace(omega=0.3)
+    opt._jk_b200 = Plan()
+    eb._get_jk(opt, 'D', 1)
+    eb._get_k(opt, 'D', 1)
+    eb._get_k(opt, 'D', 1, None, -0.2, 1.0, 0.25)
+    opt.mol = types.SimpleNamespace(omega=0.0)
+    eb._get_k(opt, 'D', 1)
+    assert seen == [('jk', 0.3), ('k', 0.3, None, None), ('k', -0.2, 1.0, 0.25),
+                    ('k', None, None, None)]
+    # the long-range operator of omega = 0.3 is one erf term
+    from electrolites_b200.jk import _rsh_terms
+    assert _rsh_terms(0.3, None, None) == [(1.0, 0.3)]
+
+
+def test_module_plan_cache_follows_the_geometry():
+    """The module functions' plan cache is keyed by the molecule's content:
+    moving an atom in place changes the key, an unchanged molecule keeps it."""
+    from electrolites_b200 import clusters
+    from electrolites_b200.jk import _opt_key
+    mol = clusters.water_mole(2, 4.0, 3, basis='6-31g*')
+    k0 = _opt_key(mol)
+    assert _opt_key(mol) == k0
+    ptr = mol._atm[0, 1]
+    mol._env[ptr] += 0.1
+    assert _opt_key(mol) != k0
+    mol._env[ptr] -= 0.1
+    assert _opt_key(mol) == k0

@@ -48,6 +48,11 @@ NMAX = 7            # up to (ff|ff): floor(12/2) + 1 roots
 # n <= 7 (10 coefficients: five 16-byte loads per row in the kernels).
 SEGMENTS = ((0.0, 20.0, 0.5), (20.0, 40.0, 1.0), (40.0, 100.0, 2.0))
 XMAX = 100.0        # tables cover [0, XMAX); the Hermite limit is used above
+# Per order n, the argument from which the kernels switch to the Hermite
+# limit: the substitution changes no root or weight by more than ~1e-16
+# relative there (check_asymptotic; the fits themselves are ~1e-14), and
+# every primitive quartet above it skips the table.
+XMAX_N = (40.0, 50.0, 56.0, 62.0, 70.0, 78.0, 86.0)
 NINT = sum(int(round((b - a) / h)) for a, b, h in SEGMENTS)
 DEGREE = 9          # Chebyshev degree per interval (DEGREE + 1 coefficients)
 DEGREE_F32 = 7      # degree of the single-precision table (mixed precision)
@@ -183,7 +188,10 @@ def rys_asymptotic(n: int, x: float):
     return r / x, W / np.sqrt(x)
 
 
-def check_asymptotic(n: int, x: float = XMAX) -> float:
+def check_asymptotic(n: int, x: float = None) -> float:
+    """Largest relative change of a root or weight of order n at x (default:
+    the order's switch point XMAX_N) when [0, 1] is replaced by [0, inf)."""
+    x = XMAX_N[n - 1] if x is None else x
     r0, w0 = rys_exact(n, x)
     r1, w1 = rys_asymptotic(n, x)
     return float(max(np.max(np.abs(r1 / r0 - 1)), np.max(np.abs(w1 / w0 - 1))))
@@ -296,7 +304,7 @@ def clenshaw(c, s):
 def eval_table(tabs, n, x):
     """Evaluate the fitted table exactly as the kernels do (float64)."""
     x = float(x)
-    if x >= XMAX:
+    if x >= XMAX_N[n - 1]:
         r, w = rys_asymptotic(n, x)
         return r.astype(np.float64), w.astype(np.float64)
     it, s = locate(x)
@@ -349,6 +357,8 @@ def write_include(outdir: str) -> None:
         f'#define RYS_DEGREE_F32 {DEGREE_F32}',
         f'#define RYS_TABLE_SIZE {off}',
         f'#define RYS_TABLE32_SIZE {off32}',
+        'template <int N> __host__ __device__ constexpr double rys_xmax()',
+        '{ return ' + ' '.join(f'N == {n + 1} ? {x!r} :' for n, x in enumerate(XMAX_N)) + ' RYS_XMAX; }',
         'template <int N> __host__ __device__ constexpr int rys_offset()',
         '{ return ' + ' '.join(f'N == {n + 1} ? {o} :' for n, o in enumerate(offs)) + ' -1; }',
         'template <int N> __host__ __device__ constexpr int rys32_offset()',

@@ -1210,10 +1210,15 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     std::vector<PairRec> recs;
     for (int k = 0; k < NPAIR_CLASSES; ++k) {
         auto &v = byclass[k];
-        // primitive-pair count first (sub-lists of equal loop bounds), then q
+        // primitive-pair count first (sub-lists of equal loop bounds), then
+        // the Schwarz bin (descending), then the shells (runs of kets that
+        // share their first shell, see JK_QBIN_W)
         std::stable_sort(v.begin(), v.end(), [&](int a, int b) {
             if (cand[a].w != cand[b].w) return cand[a].w > cand[b].w;
-            return q[a] > q[b];
+            const float ba = jk_qbin(q[a]), bb = jk_qbin(q[b]);
+            if (ba != bb) return ba > bb;
+            if (cand[a].x != cand[b].x) return cand[a].x < cand[b].x;
+            return cand[a].y < cand[b].y;
         });
         p->pc_off[k] = (int)recs.size();
         p->sub_off[k] = (int)p->subs.size();

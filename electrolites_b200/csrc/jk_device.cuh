@@ -8,7 +8,8 @@
 //                      Kp_ij = sqrt(2 pi^(5/2)) K_ij / a_ij,
 //                      P the product centre, PA = P - A.
 //   shell-pair records PairRec per shell pair, grouped by pair class
-//                      (la, lb), la >= lb, each group sorted by q descending.
+//                      (la, lb), la >= lb, each group in sub-lists of equal
+//                      primitive count ordered by Schwarz bin (JK_QBIN_W).
 //   q                  float log(sqrt(max_ab |(ab|ab)|)) per pair record.
 //   dm_cond            float log(max |D| over densities, both orientations)
 //                      per shell pair, nbas x nbas.
@@ -34,6 +35,17 @@
 // the same fields as floats, 12 per record (16-byte aligned)
 #define JK_PRIM32_STRIDE 12
 
+// Order of the pairs within a sub-list: by the decade of their Schwarz
+// bound (q / JK_QBIN_W, JK_QBIN_W = ln 10, descending), then by first and
+// second shell.  The bins keep the candidates of a bra pair a prefix of the
+// sub-list (every pair of a bin above the cut passes the Schwarz test, the
+// cut's own bin is screened per quartet); within a bin, pairs that share
+// their first shell k are adjacent, so the K_h[i,k] and K_h[j,k] terms of a
+// run of kets accumulate in registers and the density rows D[i,k], D[j,k]
+// of neighbouring lanes coincide.
+#define JK_QBIN_W 2.302585092994046f
+__host__ __device__ __forceinline__ float jk_qbin(float q) { return floorf(q / JK_QBIN_W); }
+
 struct PairRec {
     int ish, jsh;        // shells; ish carries the higher angular momentum
     int i0, j0;          // first Cartesian AO of each shell
@@ -47,7 +59,7 @@ struct PairRec {
 // of views -- one plan for an ordinary build, hundreds in a batched build --
 // and every task names the view it belongs to.
 struct PlanView {
-    const PairRec *bra;      // bra pair class of this plan (sub-lists, q desc)
+    const PairRec *bra;      // bra pair class of this plan (sub-lists, binned)
     const PairRec *ket;      // ket pair class of this plan
     const int2 *sub;         // ket sub-lists [begin, end) within the ket class
     const double *prim;      // prim-pair records of this plan

@@ -332,8 +332,9 @@ __global__ void dm_max_kernel(const CondItem *__restrict__ items, int *__restric
 
 // Rows of the task decomposition: one per (view v, bra pair b, ket sub-list
 // s), r = row0(v) + b * nsub(v) + s.  row_ncand[r] = kets of sub-list s
-// (sorted by q) that can pass the Schwarz test with the plan's largest
-// density element, limited to ket index <= b within a diagonal class.
+// (ordered by Schwarz bin) in the bins that can pass the Schwarz test with
+// the plan's largest density element, limited to ket index <= b within a
+// diagonal class.
 __global__ void task_rows_kernel(const ClassArgs a, int *__restrict__ row_ncand)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -346,7 +347,10 @@ __global__ void task_rows_kernel(const ClassArgs a, int *__restrict__ row_ncand)
     const PlanView &V = a.views[lo];
     const int rl = r - V.row0;
     const int b = rl / V.nsub, s = rl - (rl / V.nsub) * V.nsub;
-    const float cut = V.log_tol - V.bra[b].q - *V.dm_max;
+    // candidates: the kets of every Schwarz bin from the top down to the bin
+    // of the cut (pairs are sorted by bin within a sub-list; the cut's bin is
+    // screened quartet by quartet)
+    const float cut = jk_qbin(V.log_tol - V.bra[b].q - *V.dm_max);
     lo = V.sub[s].x;
     hi = V.sub[s].y;
     if (V.same_class && hi > b + 1) hi = b + 1;
@@ -354,7 +358,7 @@ __global__ void task_rows_kernel(const ClassArgs a, int *__restrict__ row_ncand)
     if (lo > hi) hi = lo;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (V.ket[mid].q > cut) lo = mid + 1; else hi = mid;
+        if (jk_qbin(V.ket[mid].q) >= cut) lo = mid + 1; else hi = mid;
     }
     row_ncand[r] = lo - first;
 }

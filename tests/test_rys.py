@@ -50,11 +50,16 @@ def test_table_fit_accuracy():
     ~1e-15 relative over [0, XMAX) and uses the exact Hermite limit above."""
     tabs = R.fit_tables(R.DEGREE, nmax=3)
     rng = np.random.default_rng(7)
-    xs = np.concatenate([rng.uniform(0, R.XMAX, 60), [0.0, 1e-10, R.XMAX - 1e-9]])
+    xs = np.concatenate([rng.uniform(0, R.XMAX, 60), [0.0, 1e-10, R.XMAX - 1e-9],
+                         [v - 1e-9 for v in R.XMAX_N[:3]], list(R.XMAX_N[:3])])
     for n in range(1, 4):
         assert R.fit_error(tabs, n, xs) < 5e-15
     for n in range(1, 8):
         assert R.check_asymptotic(n, R.XMAX) < 1e-15
+        # the kernels switch to the Hermite limit at XMAX_N[n-1] <= XMAX
+        assert R.XMAX_N[n - 1] <= R.XMAX
+        for x in (R.XMAX_N[n - 1], R.XMAX_N[n - 1] + 3.0):
+            assert R.check_asymptotic(n, x) < 5e-16
 
 
 def test_table_include_matches_fit(tmp_path):

@@ -27,7 +27,8 @@ How the numbers here are made (no table is taken from anywhere else):
   1e-16 relative (checked by `check_asymptotic`).
 * Below XMAX each of the 2n functions u_i(x), w_i(x) is fitted, per interval
   of width H, by a Chebyshev series of degree DEGREE interpolated at the
-  Chebyshev points of that interval.
+  Chebyshev points of that interval (order n: the intervals below its switch
+  point XMAX_N[n-1] only).
 
 Run as a script to write the C include file used by the CUDA build.
 """
@@ -44,18 +45,30 @@ LD = np.longdouble
 NMAX = 7            # up to (ff|ff): floor(12/2) + 1 roots
 # Interval layout of the piecewise Chebyshev fit: (start, end, width) per
 # segment.  The roots vary fastest at small x, so the intervals are narrow
-# there; degree 9 keeps every root and weight within ~1e-14 relative for
-# n <= 7 (10 coefficients: five 16-byte loads per row in the kernels).
-SEGMENTS = ((0.0, 20.0, 0.5), (20.0, 40.0, 1.0), (40.0, 100.0, 2.0))
-XMAX = 100.0        # tables cover [0, XMAX); the Hermite limit is used above
+# there; degree 7 on these widths keeps every root and weight within ~2e-15
+# relative for n <= 7 (8 coefficients: four 16-byte loads per row in the
+# kernels, the data path being what the one-root classes wait on).
+SEGMENTS = ((0.0, 10.0, 0.25), (10.0, 30.0, 0.5), (30.0, 100.0, 1.0))
+XMAX = 100.0        # the segments cover [0, XMAX)
 # Per order n, the argument from which the kernels switch to the Hermite
 # limit: the substitution changes no root or weight by more than ~1e-16
-# relative there (check_asymptotic; the fits themselves are ~1e-14), and
-# every primitive quartet above it skips the table.
+# relative there (check_asymptotic; the fits themselves are ~1e-15), and
+# every primitive quartet above it skips the table.  The table of order n
+# holds the intervals below XMAX_N[n-1] only.
 XMAX_N = (40.0, 50.0, 56.0, 62.0, 70.0, 78.0, 86.0)
 NINT = sum(int(round((b - a) / h)) for a, b, h in SEGMENTS)
-DEGREE = 9          # Chebyshev degree per interval (DEGREE + 1 coefficients)
+DEGREE = 7          # Chebyshev degree per interval (DEGREE + 1 coefficients)
 DEGREE_F32 = 7      # degree of the single-precision table (mixed precision)
+
+
+def nint(n: int) -> int:
+    """Intervals the table of order n holds: those below XMAX_N[n-1]."""
+    out = 0
+    for a, b, h in SEGMENTS:
+        if a >= XMAX_N[n - 1]:
+            break
+        out += int(round((min(b, XMAX_N[n - 1]) - a) / h))
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -246,8 +259,8 @@ def fit_tables(deg: int = DEGREE, nmax: int = NMAX):
     out = []
     ivs = intervals()
     for n in range(1, nmax + 1):
-        tab = np.zeros((len(ivs), 2 * n, m), dtype=LD)
-        for it, (a, h) in enumerate(ivs):
+        tab = np.zeros((nint(n), 2 * n, m), dtype=LD)
+        for it, (a, h) in enumerate(ivs[:nint(n)]):
             xs = LD(a) + (cheb_pts + 1) * LD(h) / 2
             vals = np.array([np.concatenate(rys_exact(n, float(xv)))
                              for xv in xs])        # (m, 2n)
@@ -336,9 +349,9 @@ def write_include(outdir: str) -> None:
     offs32, off32 = [], 0
     for n in range(1, NMAX + 1):
         offs.append(off)
-        off += NINT * 2 * n * (DEGREE + 1)
+        off += nint(n) * 2 * n * (DEGREE + 1)
         offs32.append(off32)
-        off32 += NINT * 2 * n * (DEGREE_F32 + 1)
+        off32 += nint(n) * 2 * n * (DEGREE_F32 + 1)
     dims = [
         '// Generated by electrolites_b200/codegen/rys_table.py -- do not edit.',
         '#pragma once',
@@ -359,6 +372,8 @@ def write_include(outdir: str) -> None:
         f'#define RYS_TABLE32_SIZE {off32}',
         'template <int N> __host__ __device__ constexpr double rys_xmax()',
         '{ return ' + ' '.join(f'N == {n + 1} ? {x!r} :' for n, x in enumerate(XMAX_N)) + ' RYS_XMAX; }',
+        'template <int N> __host__ __device__ constexpr int rys_nint()',
+        '{ return ' + ' '.join(f'N == {n} ? {nint(n)} :' for n in range(1, NMAX + 1)) + ' -1; }',
         'template <int N> __host__ __device__ constexpr int rys_offset()',
         '{ return ' + ' '.join(f'N == {n + 1} ? {o} :' for n, o in enumerate(offs)) + ' -1; }',
         'template <int N> __host__ __device__ constexpr int rys32_offset()',

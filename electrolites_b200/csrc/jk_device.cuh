@@ -186,16 +186,15 @@ __device__ __forceinline__ void rys_locate_f32(float x, int &it, float &s)
     s = 2.0f * (v - fk) - 1.0f;
 }
 
-// One table row, sum_k c_k s^k with k < 10, by Estrin's scheme (depth 4).
-__device__ __forceinline__ double rys_poly10(const double2 *__restrict__ cr, double s,
-                                             double s2, double s4, double s8)
+// One table row, sum_k c_k s^k with k < 8, by Estrin's scheme (depth 3).
+__device__ __forceinline__ double rys_poly8(const double2 *__restrict__ cr, double s,
+                                            double s2, double s4)
 {
     const double2 c01 = __ldg(cr), c23 = __ldg(cr + 1), c45 = __ldg(cr + 2);
-    const double2 c67 = __ldg(cr + 3), c89 = __ldg(cr + 4);
+    const double2 c67 = __ldg(cr + 3);
     const double p0 = fma(c01.y, s, c01.x), p1 = fma(c23.y, s, c23.x);
     const double p2 = fma(c45.y, s, c45.x), p3 = fma(c67.y, s, c67.x);
-    const double p4 = fma(c89.y, s, c89.x);
-    return fma(p4, s8, fma(fma(p3, s2, p2), s4, fma(p1, s2, p0)));
+    return fma(fma(p3, s2, p2), s4, fma(p1, s2, p0));
 }
 
 template <int N>
@@ -203,8 +202,8 @@ __device__ __forceinline__ void rys_roots(double x, const double *__restrict__ t
                                           double *__restrict__ r,
                                           double *__restrict__ w)
 {
-    static_assert(RYS_DEGREE == 9, "rys_poly10 evaluates degree 9");
-    if (x >= RYS_XMAX) {
+    static_assert(RYS_DEGREE == 7, "rys_poly8 evaluates degree 7");
+    if (x >= rys_xmax<N>()) {
         double ix = rsqrt(x);
         double inv = ix * ix;
 #pragma unroll
@@ -217,12 +216,12 @@ __device__ __forceinline__ void rys_roots(double x, const double *__restrict__ t
     int it;
     double s;
     rys_locate(x, it, s);
-    const double s2 = s * s, s4 = s2 * s2, s8 = s4 * s4;
+    const double s2 = s * s, s4 = s2 * s2;
     const double2 *c = reinterpret_cast<const double2 *>(
         tab + rys_offset<N>() + it * (2 * N * (RYS_DEGREE + 1)));
 #pragma unroll
     for (int row = 0; row < 2 * N; ++row) {
-        const double v = rys_poly10(c + row * (RYS_DEGREE + 1) / 2, s, s2, s4, s8);
+        const double v = rys_poly8(c + row * (RYS_DEGREE + 1) / 2, s, s2, s4);
         if (row < N) r[row] = v; else w[row - N] = v;
     }
 }

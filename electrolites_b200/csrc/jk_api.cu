@@ -224,6 +224,7 @@ struct jk_plan {
     ShellDev *d_shells = nullptr;
     double *d_basis = nullptr;
     double *d_prim = nullptr;
+    double *d_prim_soa = nullptr;   // field-major copy in ket order
     float *d_prim32 = nullptr;      // FP32 copies of the records (mixed form)
     PairRec *d_pairs = nullptr;
     int *d_sh_ao = nullptr, *d_sh_nf = nullptr;
@@ -564,6 +565,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             v.ket = p->d_pairs + p->pc_off[B];
             v.sub = p->d_subs + p->sub_off[B];
             v.prim = p->d_prim;
+            v.prim_soa = p->d_prim_soa;
             v.prim32 = p->d_prim32;
             v.dm_cond = it.dmc;
             v.dm_max = it.dm_max;
@@ -1039,6 +1041,7 @@ static void free_plan(jk_plan *p)
     cudaFree(p->d_shells);
     cudaFree(p->d_basis);
     cudaFree(p->d_prim);
+    cudaFree(p->d_prim_soa);
     cudaFree(p->d_prim32);
     cudaFree(p->d_pairs);
     cudaFree(p->d_sh_ao);
@@ -1208,6 +1211,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
         byclass[pair_class(shells[i].l, shells[j].l)].push_back((int)c);
     }
     std::vector<PairRec> recs;
+    size_t soa_total = 0, soa_block = 0;   // doubles of the field-major copy
     for (int k = 0; k < NPAIR_CLASSES; ++k) {
         auto &v = byclass[k];
         // primitive-pair count first (sub-lists of equal loop bounds), then
@@ -1228,8 +1232,18 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
             p->subs.back().y = (int)t + 1;
         }
         int mp = 0;
-        for (int c : v) {
+        size_t sub_start = 0, sub_n = 0;   // the current sub-list's block
+        for (size_t t = 0; t < v.size(); ++t) {
+            const int c = v[t];
             const int i = cand[c].x, j = cand[c].y;
+            if (t == 0 || cand[c].w != cand[v[t - 1]].w) {
+                // a new sub-list: its block follows the previous one
+                soa_total += sub_n * (size_t)(t ? cand[v[t - 1]].w : 0) * JK_SOA_FIELDS;
+                sub_start = t;
+                sub_n = 0;
+                while (sub_start + sub_n < v.size() && cand[v[sub_start + sub_n]].w == cand[c].w) ++sub_n;
+                soa_block = soa_total;
+            }
             PairRec r;
             r.ish = i;
             r.jsh = j;
@@ -1239,14 +1253,18 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
             r.nprim = cand[c].w;
             r.q = q[c];
             r.xoff = 0;       // set below, once the classes are laid out
+            r.soa = (int)std::min<size_t>(soa_block + (t - sub_start), INT_MAX);
+            r.soa_n = (int)sub_n;
             r.ABx = shells[i].x - shells[j].x;
             r.ABy = shells[i].y - shells[j].y;
             r.ABz = shells[i].z - shells[j].z;
             mp = std::max(mp, r.nprim);
             recs.push_back(r);
         }
+        if (!v.empty()) soa_total += sub_n * (size_t)cand[v.back()].w * JK_SOA_FIELDS;
         p->pc_maxprim[k] = mp;
     }
+    if (soa_total > (size_t)INT_MAX) return fail(JK_ERR_ARG, "molecule too large (primitive pairs)");
     p->pc_off[NPAIR_CLASSES] = (int)recs.size();
     // x-space blocks of the J engine in pair order: NX = sum of ncart over
     // the transfer's source levels la..la+lb
@@ -1283,6 +1301,16 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     p->max_rows = max_rows;
     p->npairs = (long long)recs.size();
     CK(upload(&p->d_pairs, recs, st, &p->table_bytes));
+    {   // the field-major copy of the primitive records, in ket order
+        const size_t bytes = std::max<size_t>(1, soa_total) * sizeof(double);
+        CK(cudaMalloc(&p->d_prim_soa, bytes));
+        p->table_bytes += bytes;
+        if (!recs.empty()) {
+            prim_soa_fill_kernel<<<(unsigned)((recs.size() + 127) / 128), 128, 0, st>>>(
+                p->d_pairs, (long long)recs.size(), p->d_prim, p->d_prim_soa);
+            CK(cudaGetLastError());
+        }
+    }
     std::vector<int> nf(nbas);
     for (int s = 0; s < nbas; ++s) nf[s] = ncart(shells[s].l);
     CK(upload(&p->d_sh_ao, p->sh_ao, st, &p->table_bytes));

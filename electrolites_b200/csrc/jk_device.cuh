@@ -52,8 +52,17 @@ struct PairRec {
     int prim0, nprim;    // first record and count in the prim-pair table
     float q;             // log Schwarz bound
     int xoff;            // first element of this pair's x-space block (J engine)
+    int soa, soa_n;      // field-major copy: field f of primitive pair k at
+                         // prim_soa[soa + (k * JK_SOA_FIELDS + f) * soa_n]
     double ABx, ABy, ABz;  // A - B, for the i -> j transfer
 };
+
+// Field-major copy of the primitive-pair records in ket order (the register
+// form's ket loop): per sub-list of n pairs of P primitive pairs each, a
+// block of P * JK_SOA_FIELDS rows of n doubles, row (k, f) holding field f
+// (PR_* order) of primitive pair k of every pair of the sub-list.  Lanes that
+// evaluate neighbouring kets of a sub-list read neighbouring doubles.
+#define JK_SOA_FIELDS 9
 
 // One plan (molecule) as one class launch sees it.  A launch covers a list
 // of views -- one plan for an ordinary build, hundreds in a batched build --
@@ -63,6 +72,7 @@ struct PlanView {
     const PairRec *ket;      // ket pair class of this plan
     const int2 *sub;         // ket sub-lists [begin, end) within the ket class
     const double *prim;      // prim-pair records of this plan
+    const double *prim_soa;  // their field-major copy in ket order
     const float *prim32;     // their FP32 copies
     const float *dm_cond;    // nbas x nbas
     const float *dm_max;     // device scalar: max of dm_cond

@@ -60,6 +60,22 @@ __global__ void prim32_fill_kernel(const double *__restrict__ prim, long long nr
     for (int f = 0; f < JK_PRIM32_STRIDE; ++f) o[f] = f < 9 ? (float)in[f] : 0.f;
 }
 
+// The field-major copy of the records (JK_SOA_FIELDS, PairRec::soa): one
+// thread per pair of the class lists
+__global__ void prim_soa_fill_kernel(const PairRec *__restrict__ pairs, long long npairs,
+                                     const double *__restrict__ prim, double *__restrict__ soa)
+{
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const PairRec r = pairs[p];
+    for (int k = 0; k < r.nprim; ++k) {
+        const double *in = prim + (size_t)(r.prim0 + k) * JK_PRIM_STRIDE;
+#pragma unroll
+        for (int f = 0; f < JK_SOA_FIELDS; ++f)
+            soa[r.soa + (size_t)(k * JK_SOA_FIELDS + f) * r.soa_n] = in[f];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Schwarz bound per shell pair: q = log sqrt(max_ab |(ab|ab)|), with a
 // runtime-l Rys evaluation (l <= 3).  One thread per pair; O(npairs) work.

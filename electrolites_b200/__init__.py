@@ -5,10 +5,14 @@ Public API:
     tables), with ``get_jk`` / ``get_k`` / ``get_j``;
   * ``jk.get_jk(mol, dm, ...)``, ``jk.get_j``, ``jk.get_k`` -- GPU4PySCF's
     module-level signatures;
+  * ``jk.jk_energy_per_atom`` / ``VHFOpt.jk_energy_per_atom`` -- the nuclear
+    gradient of the two-electron energy (GPU4PySCF's
+    ``grad.rhf._jk_energy_per_atom``);
   * ``patch(*names)`` / ``patch_all()`` -- install the engine in place of
-    GPU4PySCF's ``_VHFOpt.get_jk`` / ``get_k`` and ``j_engine._VHFOpt.get_j``,
-    the targets the reference patches (electrolites/__init__.py:59-61, 107,
-    329-350).  ``check_targets()`` reports which targets exist.
+    GPU4PySCF's ``_VHFOpt.get_jk`` / ``get_k``, ``j_engine._VHFOpt.get_j``
+    and ``grad.rhf._jk_energy_per_atom``, the targets the reference patches
+    (electrolites/__init__.py:59-61, 73, 107, 329-350).  ``check_targets()``
+    reports which targets exist.
 """
 from __future__ import annotations
 
@@ -23,6 +27,7 @@ _TARGETS = {
     'fastjk': ('gpu4pyscf.scf.jk', '_VHFOpt', 'get_jk'),
     'fastk': ('gpu4pyscf.scf.jk', '_VHFOpt', 'get_k'),
     'fastj': ('gpu4pyscf.scf.j_engine', '_VHFOpt', 'get_j'),
+    'fastejk': ('gpu4pyscf.grad.rhf', None, '_jk_energy_per_atom'),   # a module function
 }
 MODULES = tuple(_TARGETS)
 _PATCHED = {}
@@ -34,7 +39,7 @@ def check_targets():
     for name, (mod, cls, meth) in _TARGETS.items():
         try:
             m = importlib.import_module(mod)
-            c = getattr(m, cls)
+            c = m if cls is None else getattr(m, cls)
             getattr(c, meth)
             out[name] = None
         except Exception as err:   # noqa: BLE001
@@ -109,12 +114,26 @@ def _get_j(self, dms, verbose=None):
     return _out(_plan_for(self).get_j(dms, verbose), dms)
 
 
-_IMPL = {'fastjk': _get_jk, 'fastk': _get_k, 'fastj': _get_j}
+def _jk_energy_per_atom(vhfopt, dm, j_factor=1., k_factor=1., verbose=None):
+    """grad.rhf._jk_energy_per_atom: dm in the option's molecule basis,
+    brought to its sorted Cartesian basis by the option object itself (as
+    electrolites/fastejk.py:273-276 does); the operator's omega from the
+    option's molecule.  Returns a numpy (natm, 3) array."""
+    nao = vhfopt.mol.nao
+    dm = dm.reshape(-1, nao, nao) if hasattr(dm, 'reshape') else dm
+    dms = vhfopt.apply_coeff_C_mat_CT(dm)
+    omega = _resolve_omega(vhfopt, None) or 0.0
+    g = _plan_for(vhfopt).jk_energy_per_atom(dms, j_factor, k_factor, omega)
+    return g.cpu().numpy()
+
+
+_IMPL = {'fastjk': _get_jk, 'fastk': _get_k, 'fastj': _get_j,
+         'fastejk': _jk_energy_per_atom}
 
 
 def patch(*names):
     """Install the engine for the named targets ('fastjk', 'fastk',
-    'fastj').  Raises if a target does not exist (no silent partial
+    'fastj', 'fastejk').  Raises if a target does not exist (no silent partial
     patching)."""
     status = check_targets()
     for name in names:
@@ -126,7 +145,8 @@ def patch(*names):
         if name in _PATCHED:
             continue
         mod, cls, meth = _TARGETS[name]
-        c = getattr(importlib.import_module(mod), cls)
+        m = importlib.import_module(mod)
+        c = m if cls is None else getattr(m, cls)
         _PATCHED[name] = getattr(c, meth)
         setattr(c, meth, _IMPL[name])
     return list(_PATCHED)

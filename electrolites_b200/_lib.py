@@ -23,7 +23,7 @@ EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_plan_set_tol', 'jk_plan_set_jengine', 'jk_plan_set_tuning',
            'jk_batch_create', 'jk_batch_destroy', 'jk_batch_build', 'jk_batch_sync',
            'jk_batch_counts', 'jk_batch_set_timing', 'jk_batch_class_ms',
-           'jk_batch_set_tuning', 'jk_batch_stats', 'jk_last_error']
+           'jk_batch_set_tuning', 'jk_batch_stats', 'jk_last_error', 'jk_grad']
 
 _lib = None
 
@@ -56,6 +56,7 @@ def lib():
     L.jk_build_op.argtypes = [vp, dp, c_int, c_int, c_int, c_int, dp, dp, c_double, c_int, vp, vp,
                               vp]
     L.jk_sync.argtypes = [vp, vp]
+    L.jk_grad.argtypes = [vp, dp, c_int, c_double, c_double, c_double, dp, vp]
     L.jk_last_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong),
                                  ctypes.POINTER(ctypes.c_ulonglong),
                                  ctypes.POINTER(ctypes.c_ulonglong), c_int, ip]

@@ -160,10 +160,12 @@ def _scaled(n, name):
     return name if n == 1 else f'T({n}) * {name}'
 
 
-def gen_vrr(em, cls, d, zero_one):
-    """Emit G_d[e][f] for e <= lij, f <= lkl; returns dict (e, f) -> expr.
-    zero_one: the value of G_d[0][0] ('1' for x and y, 'wz' for z)."""
-    lij, lkl = cls.lij, cls.lkl
+def gen_vrr(em, cls, d, zero_one, lij=None, lkl=None):
+    """Emit G_d[e][f] for e <= lij, f <= lkl (default: the class's); returns
+    dict (e, f) -> expr.  zero_one: the value of G_d[0][0] ('1' for x and
+    y, 'wz' for z)."""
+    lij = cls.lij if lij is None else lij
+    lkl = cls.lkl if lkl is None else lkl
     g = {(0, 0): zero_one}
     for e in range(lij):
         name = f'g{d}_{e + 1}_0'
@@ -283,6 +285,133 @@ def gen_hrr(la, lb, prefix, vec):
     return em.text()
 
 
+# ----------------------------------------------------------------------
+# nuclear gradient: blocks of the (e|f) space accumulated per quartet
+# ----------------------------------------------------------------------
+def grad_rects(cls):
+    """The four (e|f)-space blocks of the gradient kernel, (name, e-levels,
+    f-levels, weight): U unweighted (the lowered shells' transfers read it),
+    RA / RB / RC weighted by 2 alpha of the primitive of shell i / j / k
+    (the raised shells').  d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x}."""
+    li, lj, lk, ll = cls.li, cls.lj, cls.lk, cls.ll
+    lij, lkl = cls.lij, cls.lkl
+    return [('U', (max(li - 1, 0), lij), (max(lk - 1, 0), lkl), None),
+            ('RA', (li + 1, lij + 1), (lk, lkl), 'wA'),
+            ('RB', (li, lij + 1), (lk, lkl), 'wB'),
+            ('RC', (li, lij), (lk + 1, lkl + 1), 'wC')]
+
+
+def _level_set(l0, l1):
+    return [(L, c) for L in range(l0, l1 + 1) for c in comps(L)]
+
+
+def gen_grad_root(cls):
+    """One Rys root's contribution to the four gradient blocks:
+    R[fi * NE_R + ei] (+)= w * G_x G_y G_z over the block's components."""
+    em = Emitter('    ')
+    lij1, lkl1 = cls.lij + 1, cls.lkl + 1
+    gx = gen_vrr(em, cls, 'x', '1', lij1, lkl1)
+    gy = gen_vrr(em, cls, 'y', '1', lij1, lkl1)
+    gz = gen_vrr(em, cls, 'z', 'wz', lij1, lkl1)
+    rects = grad_rects(cls)
+    # every (e, f) component pair of any block, once
+    members = {}
+    for name, (e0, e1), (f0, f1), w in rects:
+        E, F = _level_set(e0, e1), _level_set(f0, f1)
+        for jf, (_, fc) in enumerate(F):
+            for ie, (_, ec) in enumerate(E):
+                members.setdefault((ec, fc), []).append((name, jf * len(E) + ie, w))
+    xy_named = {}
+    n = 0
+    for (ec, fc), targets in members.items():
+        a = gx[(ec[0], fc[0])]
+        b = gy[(ec[1], fc[1])]
+        c = gz[(ec[2], fc[2])]
+        key = (ec[0], fc[0], ec[1], fc[1])
+        if a == '1' and b == '1':
+            xy = None
+        elif a == '1':
+            xy = b
+        elif b == '1':
+            xy = a
+        else:
+            if key not in xy_named:
+                nm = f'xy{len(xy_named)}'
+                em(f'const T {nm} = {a} * {b};')
+                xy_named[key] = nm
+            xy = xy_named[key]
+        pv = f'p{n}'
+        n += 1
+        em(f'const T {pv} = {c if xy is None else xy + " * " + c};')
+        for name, k, w in targets:
+            if w is None:
+                em(f'{name}[{k}] += {pv};')
+            else:
+                em(f'{name}[{k}] = fma({w}, {pv}, {name}[{k}]);')
+    return em.text()
+
+
+GRAD_STRAIGHT_MAX = 250   # component pairs up to which grad_root is straight-line code
+
+
+def grad_members(cls):
+    """The distinct (e, f) component pairs of the four gradient blocks."""
+    mem = set()
+    for _, (e0, e1), (f0, f1), _ in grad_rects(cls):
+        for _, ec in _level_set(e0, e1):
+            for _, fc in _level_set(f0, f1):
+                mem.add((ec, fc))
+    return mem
+
+
+def gen_grad_struct(cls):
+    """Lines inside the class struct for the gradient kernel: block sizes,
+    level ranges and offsets, the root accumulation (straight-line code for
+    the smaller classes; the larger ones loop, see jk_grad.cuh, which keeps
+    their compile time bounded), and the transfers of the shells raised and
+    lowered by one."""
+    li, lj, lk, ll = cls.li, cls.lj, cls.lk, cls.ll
+    lines = []
+    rects = grad_rects(cls)
+    small = len(grad_members(cls)) <= GRAD_STRAIGHT_MAX
+    lines.append(f'    static constexpr bool G_SMALL = {"true" if small else "false"};')
+    for name, (e0, e1), (f0, f1), _ in rects:
+        ne = len(_level_set(e0, e1))
+        nf = len(_level_set(f0, f1))
+        lines.append(f'    static constexpr int G_{name}_NE = {ne}, G_{name}_NF = {nf};')
+        lines.append(f'    static constexpr int G_{name}_E0 = {e0}, G_{name}_E1 = {e1}, '
+                     f'G_{name}_F0 = {f0}, G_{name}_F1 = {f1};')
+    lines.append(f'    static constexpr int G_NROOTS = {(cls.lij + cls.lkl + 1) // 2 + 1};')
+    # offsets into U of the lowered transfers' inputs
+    ue0, uf0 = max(li - 1, 0), max(lk - 1, 0)
+    def off(l0, l):
+        return sum(ncart(x) for x in range(l0, l))
+    lines.append(f'    static constexpr int G_U_E_LI = {off(ue0, li)};    // level li in U\'s e range')
+    lines.append(f'    static constexpr int G_U_F_LK = {off(uf0, lk)};    // level lk in U\'s f range')
+    tpl = 'template <class T> __device__ static __forceinline__ void'
+    if small:
+        lines.append(f'    {tpl} grad_root(T c0x, T c0y, T c0z, T cpx, T cpy, T cpz, T b00, '
+                     'T b10, T b01, T wz, T wA, T wB, T wC, T *U, T *RA, T *RB, T *RC) {')
+        lines.append(gen_grad_root(cls))
+        lines.append('    }')
+    tpl_s = ('template <class T, int SI = 1, int SO = 1> __device__ static __forceinline__ '
+             'void')
+    shifts = [('ip', li + 1, lj, 'hbi', 'AB'), ('jp', li, lj + 1, 'hbj', 'AB'),
+              ('kp', lk + 1, ll, 'hkk', 'CD')]
+    if li > 0:
+        shifts.append(('im', li - 1, lj, 'hbm', 'AB'))
+    if lj > 0:
+        shifts.append(('jm', li, lj - 1, 'hbn', 'AB'))
+    if lk > 0:
+        shifts.append(('km', lk - 1, ll, 'hkm', 'CD'))
+    for tag, la, lb, prefix, vec in shifts:
+        args = 'T ABx, T ABy, T ABz' if vec == 'AB' else 'T CDx, T CDy, T CDz'
+        lines.append(f'    {tpl_s} hrr_{tag}(const T *in, T *out, {args}) {{')
+        lines.append(gen_hrr(la, lb, prefix, vec))
+        lines.append('    }')
+    return lines
+
+
 def gen_class_header(cls):
     E = cls.eset()
     tpl = 'template <class T> __device__ static __forceinline__ void'
@@ -341,6 +470,7 @@ def gen_class_header(cls):
     lines.append(f'    {tpl_s} hrr_ket(const T *in, T *out, T CDx, T CDy, T CDz) {{')
     lines.append(gen_hrr(cls.lk, cls.ll, 'hk', 'CD'))
     lines.append('    }')
+    lines += gen_grad_struct(cls)
     lines.append('};')
     return '\n'.join(lines)
 

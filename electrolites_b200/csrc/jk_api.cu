@@ -138,6 +138,11 @@ struct ClassTune {
 
 struct Engine {
     int device = 0, num_sms = 148;
+    // nuclear-gradient build (grad != null): its output, zeroed at launch
+    double *grad = nullptr;
+    size_t grad_bytes = 0;
+    double grad_wj = 0., grad_wk = 0.;
+    const int *grad_atom = nullptr;
     // per class stream: 4 x max_rows ints (candidates, chunks, chunk prefix,
     // candidate prefix) and CUB scratch of cub_stride bytes
     int *d_rows = nullptr;
@@ -206,7 +211,8 @@ struct jk_plan {
     int device = 0;
     int nbas_user = 0, nbas = 0, nao = 0;
     bool expanded = false;          // a general contraction was split
-    std::vector<int> sh_l, sh_ao, sh_user;
+    std::vector<int> sh_l, sh_ao, sh_user, sh_atom;
+    int natm = 0;
     double tol = 1e-13;
     float log_tol = 0.f;
     // screening threshold of the builds: the plan's own or a looser one
@@ -227,7 +233,7 @@ struct jk_plan {
     double *d_prim_soa = nullptr;   // field-major copy in ket order
     float *d_prim32 = nullptr;      // FP32 copies of the records (mixed form)
     PairRec *d_pairs = nullptr;
-    int *d_sh_ao = nullptr, *d_sh_nf = nullptr;
+    int *d_sh_ao = nullptr, *d_sh_nf = nullptr, *d_sh_atom = nullptr;
     // ket sub-lists (equal primitive-pair count) per pair class
     std::vector<int2> subs;
     int sub_off[NPAIR_CLASSES + 1] = {0};
@@ -397,11 +403,25 @@ struct Spec {
     int nterm;
     double coef[2];
     double omega[2];
+    // nuclear gradient instead of J/K: weights of W (see jk_grad.cuh) and
+    // the output, natm x 3 (device)
+    int grad = 0;
+    double grad_wj = 0., grad_wk = 0.;
+    double *grad_out = nullptr;
 };
 
 static Spec coulomb_spec(int hermi, int with_j, int with_k, double mixed_threshold)
 {
-    return Spec{hermi, with_j, with_k, mixed_threshold, 1, {1.0, 0.0}, {0.0, 0.0}};
+    Spec s;
+    s.hermi = hermi;
+    s.with_j = with_j;
+    s.with_k = with_k;
+    s.mixed_threshold = mixed_threshold;
+    s.nterm = 1;
+    s.coef[0] = 1.0;
+    s.coef[1] = 0.0;
+    s.omega[0] = s.omega[1] = 0.0;
+    return s;
 }
 
 static int check_spec(const Spec &s, const char *who)
@@ -441,7 +461,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     // J engine: J of a one-plan, one-operator build outside the static
     // scratch (with K: the quartets kept for J alone)
     const bool jx = n == 1 && items[0].p && items[0].p->jengine && s.with_j && s.hermi != 2 &&
-                    s.nterm == 1 && ws_ext == nullptr;
+                    s.nterm == 1 && ws_ext == nullptr && !s.grad;
     size_t acc = 0, need = 0;
     for (int i = 0; i < n; ++i) {
         Item &it = items[i];
@@ -450,15 +470,16 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
             return fail(JK_ERR_ARG, std::string(who) + ": plan " + std::to_string(i) +
                                         " lives on another device");
         if (it.n_dm <= 0 || !it.dm) return fail(JK_ERR_ARG, std::string(who) + ": no densities");
-        if ((s.with_j && !it.vj) || (s.with_k && !it.vk))
+        if (!s.grad && ((s.with_j && !it.vj) || (s.with_k && !it.vk)))
             return fail(JK_ERR_ARG, std::string(who) + ": output is NULL");
         const size_t nao2 = (size_t)it.p->nao * it.p->nao;
         it.n_k = s.with_k ? (s.hermi == 0 ? 2 * it.n_dm : it.n_dm) : 0;
         it.n_j = (s.with_j && s.hermi != 2) ? it.n_dm : 0;
         it.n_ka = it.n_k ? it.n_dm : 0;
         it.need_t = s.with_k && s.hermi == 0;
-        it.n_kp = pair_k ? it.n_k / 2 : 0;
-        acc += align256((size_t)it.n_k * nao2 * 8) + align256((size_t)it.n_j * nao2 * 8);
+        it.n_kp = pair_k && !s.grad ? it.n_k / 2 : 0;
+        // a gradient build reads the densities but keeps no J/K accumulators
+        if (!s.grad) acc += align256((size_t)it.n_k * nao2 * 8) + align256((size_t)it.n_j * nao2 * 8);
     }
     const size_t jx_bytes = jx ? align256((size_t)items[0].n_j * items[0].p->nx_total * 8) : 0;
     acc += jx_bytes;               // the x-space J, cleared with the accumulators
@@ -500,9 +521,9 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     for (Item &it : items) {
         const size_t nao2 = (size_t)it.p->nao * it.p->nao;
         it.Kh = (double *)(ws + o);
-        o += align256((size_t)it.n_k * nao2 * 8);
+        o += s.grad ? 0 : align256((size_t)it.n_k * nao2 * 8);
         it.Jh = (double *)(ws + o);
-        o += align256((size_t)it.n_j * nao2 * 8);
+        o += s.grad ? 0 : align256((size_t)it.n_j * nao2 * 8);
     }
     E.jx = jx;
     E.jx_jonly = !s.with_k;
@@ -536,6 +557,11 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     // ---- class views ----
     const float log_mixed = s.mixed_threshold > 0 ? (float)std::log(s.mixed_threshold) : -INFINITY;
     E.mixed = s.mixed_threshold > 0;
+    E.grad = s.grad ? s.grad_out : nullptr;
+    E.grad_bytes = s.grad ? (size_t)items[0].p->natm * 3 * sizeof(double) : 0;
+    E.grad_wj = s.grad_wj;
+    E.grad_wk = s.grad_wk;
+    E.grad_atom = s.grad ? items[0].p->d_sh_atom : nullptr;
     E.nterm = s.nterm;
     for (int t = 0; t < 2; ++t) {
         const bool on = t < s.nterm;
@@ -645,10 +671,10 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
         if (it.n_j || it.need_t)   // D + D^T for J, D^T for the K of hermi 0
             pre.push_back(op(it.dm, it.dm, it.n_j ? it.dsJ : nullptr, it.need_t ? it.DT : nullptr,
                              1.0, nao, it.n_dm, pre_tiles));
-        if (s.with_j)              // J = J_h + J_h^T (zero for hermi 2)
+        if (s.with_j && !s.grad)   // J = J_h + J_h^T (zero for hermi 2)
             post.push_back(it.n_j ? op(it.Jh, it.Jh, it.vj, nullptr, 1.0, nao, it.n_dm, post_tiles)
                                   : op(nullptr, nullptr, it.vj, nullptr, 0.0, nao, it.n_dm, post_tiles));
-        if (s.with_k) {            // K = K_h(D) + K_h(D^T)^T, or K_h +- K_h^T
+        if (s.with_k && !s.grad) { // K = K_h(D) + K_h(D^T)^T, or K_h +- K_h^T
             if (s.hermi == 0)
                 post.push_back(op(it.Kh, it.Kh + (size_t)it.n_dm * nao2, it.vk, nullptr, 1.0, nao,
                                   it.n_dm, post_tiles));
@@ -763,6 +789,10 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
                : 0;
     a.jx_dens = E.jx_dens;
     a.jx_acc = E.jx_acc;
+    a.grad = E.grad;
+    a.sh_atom = E.grad_atom;
+    a.grad_wj = E.grad_wj;
+    a.grad_wk = E.grad_wk;
     a.nterm = E.nterm;
     for (int t = 0; t < 2; ++t) {
         a.op_coef[t] = E.op_coef[t];
@@ -840,6 +870,7 @@ static int engine_launch(Engine &E, cudaStream_t st, bool timing)
     const TileOp *d_post = (const TileOp *)(E.d_blob + E.off_post);
     const CondItem *d_cond = (const CondItem *)(E.d_blob + E.off_cond);
     if (E.acc_bytes) CK(cudaMemsetAsync(E.ws, 0, E.acc_bytes, st));
+    if (E.grad) CK(cudaMemsetAsync(E.grad, 0, E.grad_bytes, st));
     if (E.npre) {
         tile_op_kernel<<<(unsigned)E.pre_tiles, dim3(32, 8), 0, st>>>(d_pre, E.npre);
         CK(cudaGetLastError());
@@ -1093,6 +1124,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     p->build_tol = tol;
     p->build_log_tol = p->log_tol;
     p->nbas_user = nbas_user;
+    p->natm = natm;
     RC(engine_init(p->eng, device));
 
     // ---- shells (general contractions expanded, contraction-major) ----
@@ -1123,6 +1155,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
             p->sh_l.push_back(l);
             p->sh_ao.push_back(ao_loc[s] + c * ncart(l));
             p->sh_user.push_back(s);
+            p->sh_atom.push_back(ia);
         }
         if (nctr > 1) p->expanded = true;
     }
@@ -1315,6 +1348,7 @@ static int plan_create(const int *atm, int natm, const int *bas, int nbas_user, 
     for (int s = 0; s < nbas; ++s) nf[s] = ncart(shells[s].l);
     CK(upload(&p->d_sh_ao, p->sh_ao, st, &p->table_bytes));
     CK(upload(&p->d_sh_nf, nf, st, &p->table_bytes));
+    CK(upload(&p->d_sh_atom, p->sh_atom, st, &p->table_bytes));
     // the plan's own builds (one item) never grow these: jk_build_noalloc
     // relies on it
     RC(engine_reserve_rows(p->eng, max_rows, false, "jk_plan_create"));
@@ -1488,6 +1522,31 @@ extern "C" int jk_build_op(jk_plan *plan, const double *dm, int n_dm, int hermi,
     }
     return build_one(plan, dm, n_dm, hermi, with_j, with_k, vj, vk, mixed_threshold,
                      (cudaStream_t)stream, nullptr, 0, false, "jk_build_op", &op);
+}
+
+extern "C" int jk_grad(jk_plan *plan, const double *dm, int n_dm, double j_factor,
+                       double k_factor, double omega, double *grad, void *stream)
+{
+    if (!plan || !dm || !grad) return fail(JK_ERR_ARG, "jk_grad: null argument");
+    if (n_dm < 1 || n_dm > 2) return fail(JK_ERR_ARG, "jk_grad: n_dm must be 1 or 2");
+    if (!(omega >= 0) || !std::isfinite(omega))
+        return fail(JK_ERR_ARG, "jk_grad: omega must be finite and >= 0");
+    if (!std::isfinite(j_factor) || !std::isfinite(k_factor))
+        return fail(JK_ERR_ARG, "jk_grad: factors must be finite");
+    DeviceGuard g(plan->device);
+    std::vector<Item> items(1);
+    items[0].p = plan;
+    items[0].dm = dm;
+    items[0].n_dm = n_dm;
+    items[0].vj = items[0].vk = nullptr;
+    Spec s = coulomb_spec(1, 1, 1, 0.0);
+    s.omega[0] = omega;
+    s.grad = 1;
+    // W = fac [4 j Dt_ab Dt_cd - 4 k c sum_s (...)], c = 1/4 (one density) or 1/2
+    s.grad_wj = 4.0 * j_factor;
+    s.grad_wk = 4.0 * k_factor * (n_dm == 1 ? 0.25 : 0.5);
+    s.grad_out = grad;
+    return engine_build(plan->eng, items, s, (cudaStream_t)stream, nullptr, 0, false, "jk_grad");
 }
 
 extern "C" int jk_sync(jk_plan *plan, void *stream)

@@ -31,6 +31,7 @@
 #define PR_KP 2     // sqrt(2 pi^5/2) K_ij / a_ij
 #define PR_PX 3     // P (3)
 #define PR_PAX 6    // P - A (3)
+#define PR_AI 9     // a_i, the exponent of the first shell's primitive (gradients)
 // FP32 copy of the records for the mixed form's single-precision quartets:
 // the same fields as floats, 12 per record (16-byte aligned)
 #define JK_PRIM32_STRIDE 12
@@ -125,6 +126,12 @@ struct ClassArgs {
     int jx;
     const double *jx_dens;
     double *jx_acc;
+    // nuclear gradient (grad != null): dE/dR per atom, natm x 3, for
+    // W = fac [grad_wj Dt_ab Dt_cd - grad_wk sum_s (D_ac D_bd + D_ad D_bc)];
+    // sh_atom: the atom of every shell of the plan
+    double *grad;
+    const int *sh_atom;
+    double grad_wj, grad_wk;
     const double *rys;       // Rys table (double): polynomial part + large-x
     const float *rys32;      // Rys table (float)
     int *counter;            // task counter of this launch

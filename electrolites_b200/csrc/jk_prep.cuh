@@ -44,7 +44,7 @@ __global__ void prim_pair_fill_kernel(const int4 *__restrict__ rec, long long nr
     o[PR_PAX] = -t * abx;           // P - A
     o[PR_PAX + 1] = -t * aby;
     o[PR_PAX + 2] = -t * abz;
-    o[9] = 0.;
+    o[PR_AI] = ai;
 }
 
 // FP32 copies of the records (JK_PRIM32_STRIDE floats each) for the mixed

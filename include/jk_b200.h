@@ -153,6 +153,24 @@ int jk_build_noalloc(jk_plan *plan, const double *dm, int n_dm, int hermi,
                      int with_j, int with_k, double *vj, double *vk,
                      double mixed_threshold, void *stream);
 
+/*
+ * Nuclear gradient of the two-electron energy: grad[natm][3] (device,
+ * overwritten) = dE/dR_A of
+ *     E = j_factor/2 Tr[Dt J[Dt]] - k_factor c sum_s Tr[D_s K[D_s]],
+ * Dt = sum_s D_s, c = 1/4 for n_dm = 1 (a closed-shell total density) and
+ * 1/2 for n_dm = 2 (the two spin densities), for the symmetric densities
+ * dm[n_dm][nao][nao] (device) held fixed in the AO basis while the atoms
+ * and their basis functions move.  omega > 0 takes the long-range operator
+ * erf(omega r)/r.  Quartets are screened as by jk_build (Coulomb and
+ * exchange tests together).
+ *
+ * Replaces GPU4PySCF's _jk_energy_per_atom as the reference patches it
+ * (electrolites/fastejk.py:276-356, the factors at :308-316;
+ * electrolites/codegen/gen_ejk.py:102-144 for its kernels).
+ */
+int jk_grad(jk_plan *plan, const double *dm, int n_dm, double j_factor,
+            double k_factor, double omega, double *grad, void *stream);
+
 /* Wait for the plan's work on stream; returns JK_ERR_DEVICE if a kernel
  * raised its error flag (the flag is then cleared). */
 int jk_sync(jk_plan *plan, void *stream);

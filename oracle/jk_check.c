@@ -884,3 +884,395 @@ int check_eri_shells(const int *atm, const int *bas, int nbas, const double *env
     basis_free(&B);
     return err;
 }
+
+/* ====================================================================== */
+/* Nuclear gradient of the two-electron energy                             */
+/* ====================================================================== */
+/*
+ * E(R) = j/2 Tr[Dt J[Dt]] - k c sum_s Tr[D_s K[D_s]] for symmetric densities
+ * D_s (s < n_dm), Dt = sum_s D_s, c = 1/4 for one density and 1/2 for two,
+ * held fixed in the AO basis while the atoms (and their basis functions)
+ * move: the quantity GPU4PySCF's _jk_energy_per_atom returns per atom, which
+ * the reference replaces (electrolites/fastejk.py:276-356; its factor
+ * conventions at :308-316).
+ *
+ * Over the distinct permutations of a unique shell quartet (ij|kl) with
+ * degeneracy factor sf, E collects sum_abcd W_abcd (ab|cd) with
+ *   W = sf [4 j Dt_ab Dt_cd - 4 k c sum_s (D_s,ac D_s,bd + D_s,ad D_s,bc)],
+ * and the derivative of a Cartesian Gaussian on centre A,
+ *   d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x},
+ * turns d(ab|cd)/dA into integrals over the shell raised by one (its
+ * coefficients times 2 alpha) and lowered by one.  The centres of i, j and k
+ * are differentiated this way; l follows from translational invariance,
+ * dD = -(dA + dB + dC).  The integrals of the raised and lowered shells
+ * (up to g) come from a generic-l restatement of quartet() below.
+ */
+#define GL_LEV 8                   /* Cartesian levels 0..7 (g + f on one pair) */
+static int gcc[GL_LEV][36][3];
+static int gidx[GL_LEV][GL_LEV][GL_LEV];
+static int gcomps_ready = 0;
+
+static void gcomps_init(void)
+{
+    if (gcomps_ready) return;
+#pragma omp critical(gcomps_init)
+    {
+        if (!gcomps_ready) {
+            for (int L = 0; L < GL_LEV; ++L) {
+                int n = 0;
+                for (int lx = L; lx >= 0; --lx)
+                    for (int ly = L - lx; ly >= 0; --ly, ++n) {
+                        gcc[L][n][0] = lx;
+                        gcc[L][n][1] = ly;
+                        gcc[L][n][2] = L - lx - ly;
+                        gidx[lx][ly][L - lx - ly] = n;
+                    }
+            }
+            __atomic_store_n(&gcomps_ready, 1, __ATOMIC_RELEASE);
+        }
+    }
+}
+
+/* hrr() for levels up to 7 */
+static void ghrr(const double *in, int is, int l1, int l2, const double R[3], double *out, int os)
+{
+    if (l2 == 0) {
+        for (int a = 0; a < NCART(l1); ++a) out[a * os] = in[a * is];
+        return;
+    }
+    double cur[GL_LEV][160], nxt[GL_LEV][160];
+    int off = 0;
+    for (int la = l1; la <= l1 + l2; ++la) {
+        for (int a = 0; a < NCART(la); ++a) cur[la - l1][a] = in[(off + a) * is];
+        off += NCART(la);
+    }
+    for (int m = 0; m < l2; ++m) {
+        const int nbo = NCART(m), nbn = NCART(m + 1);
+        for (int la = l1; la <= l1 + l2 - m - 1; ++la) {
+            const int na = NCART(la);
+            for (int b = 0; b < nbn; ++b) {
+                const int *bc = gcc[m + 1][b];
+                const int d = bc[0] ? 0 : (bc[1] ? 1 : 2);
+                int bp[3] = {bc[0], bc[1], bc[2]};
+                bp[d] -= 1;
+                const int bo = gidx[bp[0]][bp[1]][bp[2]];
+                for (int a = 0; a < na; ++a) {
+                    const int *ac = gcc[la][a];
+                    int ap[3] = {ac[0], ac[1], ac[2]};
+                    ap[d] += 1;
+                    const int a1 = gidx[ap[0]][ap[1]][ap[2]];
+                    nxt[la - l1][a * nbn + b] = cur[la + 1 - l1][a1 * nbo + bo] +
+                                                R[d] * cur[la - l1][a * nbo + bo];
+                }
+            }
+        }
+        for (int la = l1; la <= l1 + l2 - m - 1; ++la)
+            memcpy(cur[la - l1], nxt[la - l1], sizeof(double) * NCART(la) * nbn);
+    }
+    const int nb = NCART(l2);
+    for (int a = 0; a < NCART(l1); ++a)
+        for (int b = 0; b < nb; ++b) out[(a * nb + b) * os] = cur[0][a * nb + b];
+}
+
+typedef struct {
+    double acc[100 * 100];
+    double tb[100 * 150];
+    PrimPair pa[32 * 32], pb[32 * 32];
+} GWork;
+
+static int pair_prims(const CShell *a, const CShell *b, PrimPair *out)
+{
+    const double AB[3] = {a->r[0] - b->r[0], a->r[1] - b->r[1], a->r[2] - b->r[2]};
+    const double rr = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    int np = 0;
+    for (int p = 0; p < a->nprim; ++p)
+        for (int q = 0; q < b->nprim; ++q) {
+            const double ea = a->exps[p], eb = b->exps[q], s = ea + eb, mu = ea * eb / s;
+            if (mu * rr > PRIM_EXP_CUTOFF) continue;
+            PrimPair *pp = out + np++;
+            pp->a = s;
+            pp->ha = 0.5 / s;
+            pp->px = (ea * a->r[0] + eb * b->r[0]) / s;
+            pp->py = (ea * a->r[1] + eb * b->r[1]) / s;
+            pp->pz = (ea * a->r[2] + eb * b->r[2]) / s;
+            pp->k = exp(-mu * rr) * a->coef[p] * b->coef[q] / s;
+        }
+    return np;
+}
+
+/* (ij|kl) of four shells of any l <= 4 (and l_i + l_j <= 7),
+ * out[((a * nj + b) * nk + c) * nl + d] */
+static void eri_generic(const CShell *si, const CShell *sj, const CShell *sk, const CShell *sl,
+                        double omega, GWork *W, double *out)
+{
+    const int li = si->l, lj = sj->l, lk = sk->l, ll = sl->l;
+    const int lij = li + lj, lkl = lk + ll;
+    const int nroots = (lij + lkl) / 2 + 1;
+    const int NF1 = lkl + 1;
+    int nE = 0, nF = 0;
+    for (int e = li; e <= lij; ++e) nE += NCART(e);
+    for (int f = lk; f <= lkl; ++f) nF += NCART(f);
+    double *acc = W->acc;
+    memset(acc, 0, sizeof(double) * nE * nF);
+    const int nb = pair_prims(si, sj, W->pa), nk = pair_prims(sk, sl, W->pb);
+    const double PI_FAC = 2.0 * 17.493418327624862846;
+    const double om2 = omega > 0 ? omega * omega : 0;
+    double r[CHK_NMAX], w[CHK_NMAX], g[3][GL_LEV * GL_LEV];
+    for (int pp = 0; pp < nb; ++pp) {
+        const PrimPair *P = W->pa + pp;
+        const double ap = P->a;
+        const double PA[3] = {P->px - si->r[0], P->py - si->r[1], P->pz - si->r[2]};
+        for (int qq = 0; qq < nk; ++qq) {
+            const PrimPair *Q = W->pb + qq;
+            const double aq = Q->a;
+            const double QC[3] = {Q->px - sk->r[0], Q->py - sk->r[1], Q->pz - sk->r[2]};
+            const double PQ[3] = {P->px - Q->px, P->py - Q->py, P->pz - Q->pz};
+            const double is = 1.0 / (ap + aq);
+            const double rho = ap * aq * is;
+            double theta = 1.0, x = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+            double fac = PI_FAC * P->k * Q->k * sqrt(is);
+            if (om2 > 0) {
+                theta = om2 / (om2 + rho);
+                x *= theta;
+                fac *= sqrt(theta);
+            }
+            chk_rys(nroots, x, r, w);
+            const double aqi = aq * is, api = ap * is;
+            for (int n = 0; n < nroots; ++n) {
+                const double u = theta * r[n];
+                const double b00 = 0.5 * u * is;
+                const double b10 = (1 - aqi * u) * P->ha;
+                const double b01 = (1 - api * u) * Q->ha;
+                for (int d = 0; d < 3; ++d) {
+                    const double c00 = PA[d] - aqi * u * PQ[d];
+                    const double cp00 = QC[d] + api * u * PQ[d];
+                    double *gd = g[d];
+                    gd[0] = d == 2 ? fac * w[n] : 1.0;
+                    if (lij > 0) gd[NF1] = c00 * gd[0];
+                    for (int e = 1; e < lij; ++e)
+                        gd[(e + 1) * NF1] = c00 * gd[e * NF1] + e * b10 * gd[(e - 1) * NF1];
+                    for (int f = 0; f < lkl; ++f) {
+                        gd[f + 1] = cp00 * gd[f] + (f ? f * b01 * gd[f - 1] : 0);
+                        for (int e = 1; e <= lij; ++e)
+                            gd[e * NF1 + f + 1] = cp00 * gd[e * NF1 + f] +
+                                                  (f ? f * b01 * gd[e * NF1 + f - 1] : 0) +
+                                                  e * b00 * gd[(e - 1) * NF1 + f];
+                    }
+                }
+                double *a = acc;
+                for (int fl = lk; fl <= lkl; ++fl)
+                    for (int fc = 0; fc < NCART(fl); ++fc, a += nE) {
+                        const int fx = gcc[fl][fc][0], fy = gcc[fl][fc][1], fz = gcc[fl][fc][2];
+                        int e = 0;
+                        for (int el = li; el <= lij; ++el)
+                            for (int ec = 0; ec < NCART(el); ++ec, ++e)
+                                a[e] += g[0][gcc[el][ec][0] * NF1 + fx] * g[1][gcc[el][ec][1] * NF1 + fy] *
+                                        g[2][gcc[el][ec][2] * NF1 + fz];
+                    }
+            }
+        }
+    }
+    const double AB[3] = {si->r[0] - sj->r[0], si->r[1] - sj->r[1], si->r[2] - sj->r[2]};
+    const double CD[3] = {sk->r[0] - sl->r[0], sk->r[1] - sl->r[1], sk->r[2] - sl->r[2]};
+    const int nij = NCART(li) * NCART(lj), nkl = NCART(lk) * NCART(ll);
+    for (int f = 0; f < nF; ++f) ghrr(acc + f * nE, 1, li, lj, AB, W->tb + f * nij, 1);
+    for (int ij = 0; ij < nij; ++ij) ghrr(W->tb + ij, nij, lk, ll, CD, out + ij * nkl, 1);
+}
+
+/* a shell raised (coefficients times 2 alpha) or lowered by one level */
+static CShell shell_shift(const CShell *s, int up)
+{
+    CShell t = *s;
+    t.l = s->l + (up ? 1 : -1);
+    if (up)
+        for (int p = 0; p < s->nprim; ++p) t.coef[p] = s->coef[p] * 2.0 * s->exps[p];
+    return t;
+}
+
+/*
+ * d/dR of the quartet's share of E along the centre of shell position pos
+ * (0: i, 1: j, 2: k): g[x] = sum_abcd W_abcd [P(.. idx+1x ..) - n_x M(.. idx-1x ..)],
+ * P and M the integrals with that shell raised and lowered.
+ */
+static void quartet_grad_centre(const CShell *s4[4], int pos, const double *Wt, double omega,
+                                GWork *W, double *bufP, double *bufM, double g[3])
+{
+    const CShell *sh[4] = {s4[0], s4[1], s4[2], s4[3]};
+    const int n[4] = {NCART(s4[0]->l), NCART(s4[1]->l), NCART(s4[2]->l), NCART(s4[3]->l)};
+    const CShell up = shell_shift(s4[pos], 1);
+    sh[pos] = &up;
+    eri_generic(sh[0], sh[1], sh[2], sh[3], omega, W, bufP);
+    const int lm = s4[pos]->l;
+    CShell dn;
+    if (lm > 0) {
+        dn = shell_shift(s4[pos], 0);
+        sh[pos] = &dn;
+        eri_generic(sh[0], sh[1], sh[2], sh[3], omega, W, bufM);
+    }
+    int np[4] = {n[0], n[1], n[2], n[3]}, nm[4] = {n[0], n[1], n[2], n[3]};
+    np[pos] = NCART(lm + 1);
+    nm[pos] = lm > 0 ? NCART(lm - 1) : 1;
+    g[0] = g[1] = g[2] = 0;
+    int idx[4];
+    for (idx[0] = 0; idx[0] < n[0]; ++idx[0])
+        for (idx[1] = 0; idx[1] < n[1]; ++idx[1])
+            for (idx[2] = 0; idx[2] < n[2]; ++idx[2])
+                for (idx[3] = 0; idx[3] < n[3]; ++idx[3]) {
+                    const double w = Wt[((idx[0] * n[1] + idx[1]) * n[2] + idx[2]) * n[3] + idx[3]];
+                    if (w == 0) continue;
+                    const int *c = gcc[lm][idx[pos]];
+                    for (int x = 0; x < 3; ++x) {
+                        int cu[3] = {c[0], c[1], c[2]};
+                        cu[x] += 1;
+                        int t[4] = {idx[0], idx[1], idx[2], idx[3]};
+                        t[pos] = gidx[cu[0]][cu[1]][cu[2]];
+                        double v = bufP[((t[0] * np[1] + t[1]) * np[2] + t[2]) * np[3] + t[3]];
+                        if (c[x] > 0) {
+                            int cd[3] = {c[0], c[1], c[2]};
+                            cd[x] -= 1;
+                            t[pos] = gidx[cd[0]][cd[1]][cd[2]];
+                            v -= c[x] * bufM[((t[0] * nm[1] + t[1]) * nm[2] + t[2]) * nm[3] + t[3]];
+                        }
+                        g[x] += w * v;
+                    }
+                }
+}
+
+/*
+ * grad[natm][3] = dE/dR of E = j/2 Tr[Dt J[Dt]] - k c sum_s Tr[D_s K[D_s]]
+ * (symmetric dm[n_dm][nao][nao], n_dm 1 or 2, c = 1/4 or 1/2), quartets
+ * screened as check_jk screens them (tol <= 0: none).  Returns 0 on success.
+ */
+int check_grad_jk(const int *atm, int natm, const int *bas, int nbas, const double *env,
+                  const int *ao_loc, const double *dm, int n_dm, double tol, double j_factor,
+                  double k_factor, double omega, int nthreads, double *grad,
+                  long long *nquartets)
+{
+    chk_rys_init();
+    comps_init();
+    gcomps_init();
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    if (n_dm < 1 || n_dm > 2) return 3;
+    Basis B;
+    int err = basis_load(&B, atm, bas, nbas, env, ao_loc, 0.0);
+    if (err) {
+        basis_free(&B);
+        return err;
+    }
+    for (int s = 0; s < nbas; ++s)
+        if (B.sh[s].l > 3) {
+            basis_free(&B);
+            return 1;
+        }
+    const int nao = B.nao;
+    const size_t nao2 = (size_t)nao * nao;
+    schwarz(&B);
+    const int screen = tol > 0;
+    const double log_tol = screen ? log(tol) : 0;
+    const double cK = n_dm == 1 ? 0.25 : 0.5;
+    double *dmc = malloc(sizeof(double) * nbas * nbas);
+    double *dt = malloc(sizeof(double) * nao2);
+    for (size_t x = 0; x < nao2; ++x) {
+        double v = 0;
+        for (int d = 0; d < n_dm; ++d) v += dm[d * nao2 + x];
+        dt[x] = v;
+    }
+    double dmax_all = -HUGE_VAL;
+    for (int i = 0; i < nbas; ++i)
+        for (int j = 0; j < nbas; ++j) {
+            double m = 0;
+            for (int d = 0; d < n_dm; ++d)
+                for (int a = ao_loc[i]; a < ao_loc[i + 1]; ++a)
+                    for (int b = ao_loc[j]; b < ao_loc[j + 1]; ++b) {
+                        const double v1 = fabs(dm[d * nao2 + (size_t)a * nao + b]);
+                        const double v2 = fabs(dm[d * nao2 + (size_t)b * nao + a]);
+                        if (v1 > m) m = v1;
+                        if (v2 > m) m = v2;
+                    }
+            dmc[i * nbas + j] = m > 0 ? log(m) : -HUGE_VAL;
+            if (dmc[i * nbas + j] > dmax_all) dmax_all = dmc[i * nbas + j];
+        }
+    int nthr = 1;
+#ifdef _OPENMP
+    nthr = omp_get_max_threads();
+#endif
+    double *gt = calloc((size_t)nthr * natm * 3, sizeof(double));
+    long long count = 0;
+#pragma omp parallel reduction(+:count)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double *myg = gt + (size_t)tid * natm * 3;
+        GWork *W = malloc(sizeof(GWork));
+        double *Wt = malloc(sizeof(double) * 10000);
+        double *bP = malloc(sizeof(double) * 15 * 1000), *bM = malloc(sizeof(double) * 6 * 1000);
+#pragma omp for schedule(dynamic, 4)
+        for (int pij = 0; pij < B.npair; ++pij) {
+            const ShellPair *bra = B.pairs + pij;
+            if (bra->np == 0) continue;
+            for (int pkl = 0; pkl <= pij; ++pkl) {
+                const ShellPair *ket = B.pairs + pkl;
+                if (ket->np == 0) continue;
+                const int i = bra->ish, j = bra->jsh, k = ket->ish, l = ket->jsh;
+                if (screen) {
+                    double dmax = dmc[i * nbas + j];
+                    const double c[5] = {dmc[k * nbas + l], dmc[i * nbas + k], dmc[i * nbas + l],
+                                         dmc[j * nbas + k], dmc[j * nbas + l]};
+                    for (int u = 0; u < 5; ++u) if (c[u] > dmax) dmax = c[u];
+                    if (bra->q + ket->q + dmax <= log_tol) continue;
+                }
+                count++;
+                const CShell *s4[4] = {B.sh + i, B.sh + j, B.sh + k, B.sh + l};
+                const int ni = NCART(s4[0]->l), nj = NCART(s4[1]->l);
+                const int nk = NCART(s4[2]->l), nl = NCART(s4[3]->l);
+                const int pi = bra->ish == bra->jsh, pk = ket->ish == ket->jsh;
+                const double sf = (pi ? 0.5 : 1.0) * (pk ? 0.5 : 1.0) * (pij == pkl ? 0.5 : 1.0);
+                int t = 0;
+                for (int a = 0; a < ni; ++a)
+                    for (int b = 0; b < nj; ++b)
+                        for (int c = 0; c < nk; ++c)
+                            for (int d = 0; d < nl; ++d, ++t) {
+                                const size_t A_ = s4[0]->ao0 + a, B_ = s4[1]->ao0 + b;
+                                const size_t C_ = s4[2]->ao0 + c, D_ = s4[3]->ao0 + d;
+                                double v = 4 * j_factor * dt[A_ * nao + B_] * dt[C_ * nao + D_];
+                                for (int s = 0; s < n_dm; ++s) {
+                                    const double *Ds = dm + s * nao2;
+                                    v -= 4 * k_factor * cK *
+                                         (Ds[A_ * nao + C_] * Ds[B_ * nao + D_] +
+                                          Ds[A_ * nao + D_] * Ds[B_ * nao + C_]);
+                                }
+                                Wt[t] = sf * v;
+                            }
+                double gsum[3] = {0, 0, 0};
+                for (int pos = 0; pos < 3; ++pos) {
+                    double g[3];
+                    quartet_grad_centre(s4, pos, Wt, omega, W, bP, bM, g);
+                    for (int x = 0; x < 3; ++x) {
+                        myg[s4[pos]->atom * 3 + x] += g[x];
+                        gsum[x] += g[x];
+                    }
+                }
+                for (int x = 0; x < 3; ++x) myg[s4[3]->atom * 3 + x] -= gsum[x];
+            }
+        }
+        free(W);
+        free(Wt);
+        free(bP);
+        free(bM);
+    }
+    for (int a = 0; a < natm * 3; ++a) {
+        double v = 0;
+        for (int t = 0; t < nthr; ++t) v += gt[(size_t)t * natm * 3 + a];
+        grad[a] = v;
+    }
+    if (nquartets) *nquartets = count;
+    free(gt);
+    free(dmc);
+    free(dt);
+    basis_free(&B);
+    return 0;
+}

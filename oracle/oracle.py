@@ -207,3 +207,46 @@ def jk_fast(mol, dms, tol=1e-13, with_j=True, with_k=True, nthreads=0, omega=0.0
     if squeeze:
         vj, vk = vj[0], vk[0]
     return (vj, vk, nq.value, q) if want_q else (vj, vk, nq.value)
+
+
+def grad_jk_fast(mol, dms, j_factor=1.0, k_factor=1.0, tol=1e-13, nthreads=0, omega=0.0):
+    """(grad[natm, 3], n_quartets): dE/dR per atom of
+    E = j/2 Tr[Dt J[Dt]] - k c sum_s Tr[D_s K[D_s]] (Dt = sum_s D_s, c = 1/4 for
+    one density, 1/2 for two), densities symmetric and fixed in the AO basis,
+    from the checker's analytic derivative integrals."""
+    atm, bas, env = _arrays(mol)
+    dms = np.ascontiguousarray(dms, dtype=np.float64)
+    if dms.ndim == 2:
+        dms = dms[None]
+    ao_loc = np.ascontiguousarray(mol.ao_loc_nr(cart=True), dtype=np.int32)
+    L = _check_lib()
+    if not getattr(L, '_grad_ready', False):
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.check_grad_jk.argtypes = [ip, ctypes.c_int, ip, ctypes.c_int, dp, ip, dp, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, dp,
+                                    ctypes.POINTER(ctypes.c_longlong)]
+        L._grad_ready = True
+    g = np.zeros((mol.natm, 3))
+    nq = ctypes.c_longlong(0)
+    err = L.check_grad_jk(_p(atm, ctypes.c_int), mol.natm, _p(bas, ctypes.c_int), mol.nbas,
+                          _p(env), _p(ao_loc, ctypes.c_int), _p(dms), dms.shape[0], float(tol),
+                          float(j_factor), float(k_factor), float(omega), int(nthreads), _p(g),
+                          ctypes.byref(nq))
+    if err:
+        raise RuntimeError(f'check_grad_jk failed ({err})')
+    return g, nq.value
+
+
+def jk_energy(mol, dms, j_factor=1.0, k_factor=1.0, tol=1e-13, omega=0.0):
+    """E = j/2 Tr[Dt J[Dt]] - k c sum_s Tr[D_s K[D_s]] from the checker's J/K."""
+    dms = np.asarray(dms, dtype=np.float64)
+    if dms.ndim == 2:
+        dms = dms[None]
+    vj, vk, _ = jk_fast(mol, dms, tol=tol, omega=omega)
+    dt = dms.sum(axis=0)
+    c = 0.25 if dms.shape[0] == 1 else 0.5
+    ej = 0.5 * np.einsum('ij,ji->', dt, vj.sum(axis=0))
+    ek = sum(np.einsum('ij,ji->', dms[s], vk[s]) for s in range(dms.shape[0]))
+    return j_factor * ej - k_factor * c * ek

@@ -117,3 +117,40 @@ def test_checker_shards_sum_to_the_full_build(oracle):
         sj, sk, snq = sj + a, sk + b, snq + n
     assert snq == nq
     assert np.abs(sj - fj).max() <= 1e-13 and np.abs(sk - fk).max() <= 1e-13
+
+
+def _fd_gradient(oracle, mol, dms, jf, kf, atoms, h=2e-3):
+    """Richardson-extrapolated central differences of the checker's energy
+    E = j/2 Tr[Dt J[Dt]] - k c sum_s Tr[D_s K[D_s]] at displaced atoms."""
+    g = np.zeros((len(atoms), 3))
+    for ia, A in enumerate(atoms):
+        ptr = mol._atm[A, 1]
+        for x in range(3):
+            e = {}
+            for s in (-2, -1, 1, 2):
+                mol._env[ptr + x] += s * h
+                e[s] = oracle.jk_energy(mol, dms, jf, kf, tol=0)
+                mol._env[ptr + x] -= s * h
+            d1 = (e[1] - e[-1]) / (2 * h)
+            d2 = (e[2] - e[-2]) / (4 * h)
+            g[ia, x] = (4 * d1 - d2) / 3
+    return g
+
+
+@pytest.mark.parametrize('name', ['spdf', 'h2o2'])
+def test_checker_gradient_matches_finite_differences(oracle, name):
+    """The checker's nuclear gradient of the two-electron energy (derivative
+    integrals from raised and lowered shells, up to g) against finite
+    differences of its own J/K energies, RHF- and UHF-shaped, J and K terms
+    apart; the forces sum to zero (translational invariance)."""
+    mol = {'spdf': all_class_mol,
+           'h2o2': lambda: clusters.water_mole(2, 4.0, 3, basis='6-31g*')}[name]()
+    rng = np.random.default_rng(0)
+    D = clusters.atomic_density(mol, 1) + 0.05 * rng.standard_normal((mol.nao_cart,) * 2)
+    D = 0.5 * (D + D.T)
+    for dms, jf, kf in [(D[None], 1.0, 0.2), (clusters.uhf_pair(D, 2), 1.0, 0.5),
+                        (D[None], 0.0, 1.0)]:
+        g, _ = oracle.grad_jk_fast(mol, dms, jf, kf, tol=0)
+        fd = _fd_gradient(oracle, mol, dms, jf, kf, [0, 1])
+        assert np.abs(g[:2] - fd).max() <= 1e-9 * max(1.0, np.abs(g).max())
+        assert np.abs(g.sum(axis=0)).max() <= 1e-12

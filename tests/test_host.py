@@ -126,8 +126,12 @@ def test_patch_registry(monkeypatch):
             return 'orig'
 
     jkm._VHFOpt, jem._VHFOpt = Opt, OptJ
+    grad = types.ModuleType('gpu4pyscf.grad')
+    grm = types.ModuleType('gpu4pyscf.grad.rhf')
+    grm._jk_energy_per_atom = lambda vhfopt, dm, j_factor=1., k_factor=1., verbose=None: 'orig'
     for name, m in [('gpu4pyscf', pkg), ('gpu4pyscf.scf', scf), ('gpu4pyscf.scf.jk', jkm),
-                    ('gpu4pyscf.scf.j_engine', jem)]:
+                    ('gpu4pyscf.scf.j_engine', jem), ('gpu4pyscf.grad', grad),
+                    ('gpu4pyscf.grad.rhf', grm)]:
         monkeypatch.setitem(sys.modules, name, m)
     monkeypatch.setattr(eb, '_PATCHED', {})
     assert all(v is None for v in eb.check_targets().values())
@@ -136,6 +140,7 @@ def test_patch_registry(monkeypatch):
     eb.patch_all()
     assert eb.patched() == sorted(eb.MODULES)
     assert Opt.get_jk is eb._get_jk and OptJ.get_j is eb._get_j
+    assert grm._jk_energy_per_atom is eb._jk_energy_per_atom
 
 
 def test_flop_model_counts():

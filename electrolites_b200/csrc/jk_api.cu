@@ -791,6 +791,7 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     a.jx_acc = E.jx_acc;
     a.grad = E.grad;
     a.sh_atom = E.grad_atom;
+    a.natm = E.grad ? (int)(E.grad_bytes / (3 * sizeof(double))) : 0;
     a.grad_wj = E.grad_wj;
     a.grad_wk = E.grad_wk;
     a.nterm = E.nterm;

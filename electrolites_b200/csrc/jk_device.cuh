@@ -132,6 +132,8 @@ struct ClassArgs {
     double *grad;
     const int *sh_atom;
     double grad_wj, grad_wk;
+    int natm;            // atoms of the plan (forces of up to JK_GRAD_SMEM_ATOMS
+                         // atoms are summed per block in shared memory)
     const double *rys;       // Rys table (double): polynomial part + large-x
     const float *rys32;      // Rys table (float)
     int *counter;            // task counter of this launch

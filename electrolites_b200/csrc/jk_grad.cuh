@@ -16,7 +16,11 @@
 // dD = -(dA + dB + dC).
 //
 // Work decomposition: the register form's (tasks of a bra pair against a
-// range of kets, one quartet per lane, claimed per warp).  Per quartet and
+// range of kets, one quartet per lane, claimed per warp).  Forces are summed
+// per block in shared memory (molecules of up to JK_GRAD_SMEM_ATOMS atoms)
+// and added to the output once per block and atom component: every quartet
+// adds to the same natm x 3 numbers, so global atomics per quartet would all
+// contend for a few hundred addresses.  Per quartet and
 // primitive quartet and Rys root, the code generator's grad_root adds the
 // root's 2D-integral products to four (e|f)-space blocks in registers: U
 // (unweighted), RA, RB, RC (weighted by 2 alpha of the primitive of shell i,
@@ -25,6 +29,10 @@
 // The bra atoms' forces add up in registers over a task; the ket atoms'
 // go to memory per quartet.
 #pragma once
+
+// atoms whose forces a block sums in shared memory (24 KB) before adding
+// them to the output; larger molecules add every quartet's forces there
+#define JK_GRAD_SMEM_ATOMS 1024
 
 __host__ __device__ constexpr int g_ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
@@ -131,7 +139,7 @@ __device__ __forceinline__ void grad_bra_block(const double *R, int ne, HB hb,
 template <class C>
 __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView &V,
                                              const PairRec &br, const double *__restrict__ sbra,
-                                             int entry, double sym, double gb[6])
+                                             int entry, double sym, double gb[6], double *fsum)
 {
         constexpr int LI = C::LI, LJ = C::LJ, LK = C::LK, LL = C::LL;
     constexpr int NI = C::NI, NJ = C::NJ, NK = C::NK, NL = C::NL;
@@ -324,8 +332,8 @@ __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView 
     const int ak = A.sh_atom[kt.ish], al = A.sh_atom[kt.jsh];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-        atomicAdd(A.grad + ak * 3 + x, gC[x]);
-        atomicAdd(A.grad + al * 3 + x, -(gA[x] + gB[x] + gC[x]));
+        atomicAdd(fsum + ak * 3 + x, gC[x]);
+        atomicAdd(fsum + al * 3 + x, -(gA[x] + gB[x] + gC[x]));
     }
 }
 
@@ -409,7 +417,8 @@ __device__ __noinline__ void grad_team_table(double c0, double cp, double b00, d
 template <class C>
 __device__ __forceinline__ void grad_team_quartet(const ClassArgs &A, const PlanView &V,
                                                   const PairRec &br, const double *__restrict__ sbra,
-                                                  int entry, double sym, double *ws, int lane)
+                                                  int entry, double sym, double *ws, int lane,
+                                                  double *fsum)
 {
     using T = GradTeam<C>;
     constexpr int NR = T::NR, NJ = C::NJ, NK = C::NK, NL = C::NL, NKL = NK * NL;
@@ -517,10 +526,10 @@ __device__ __forceinline__ void grad_team_quartet(const ClassArgs &A, const Plan
         const int al = A.sh_atom[kt.jsh];
 #pragma unroll
         for (int x3 = 0; x3 < 3; ++x3) {
-            atomicAdd(A.grad + at[0] * 3 + x3, g9[x3]);
-            atomicAdd(A.grad + at[1] * 3 + x3, g9[3 + x3]);
-            atomicAdd(A.grad + at[2] * 3 + x3, g9[6 + x3]);
-            atomicAdd(A.grad + al * 3 + x3, -(g9[x3] + g9[3 + x3] + g9[6 + x3]));
+            atomicAdd(fsum + at[0] * 3 + x3, g9[x3]);
+            atomicAdd(fsum + at[1] * 3 + x3, g9[3 + x3]);
+            atomicAdd(fsum + at[2] * 3 + x3, g9[6 + x3]);
+            atomicAdd(fsum + al * 3 + x3, -(g9[x3] + g9[3 + x3] + g9[6 + x3]));
         }
     }
 }
@@ -528,7 +537,7 @@ __device__ __forceinline__ void grad_team_quartet(const ClassArgs &A, const Plan
 // one task: bra pair task.bra against kets [task.k0, task.k1)
 template <class C>
 __device__ __forceinline__ void grad_task(const ClassArgs &A, const PlanView &V, const Task &task,
-                                          RegWarp &w, double *ws, int lane)
+                                          RegWarp &w, double *ws, int lane, double *fsum)
 {
     const int b = task.bra;
     const PairRec br = V.bra[b];
@@ -549,14 +558,14 @@ __device__ __forceinline__ void grad_task(const ClassArgs &A, const PlanView &V,
         if constexpr (C::G_SMALL) {
             if (lane < n) {
                 const int e2 = q[lane], k2 = e2 & JK_Q_KET;
-                grad_quartet<C>(A, V, br, w.sbra, e2, diag && k2 == b ? 0.5 * sym_b : sym_b, gb);
+                grad_quartet<C>(A, V, br, w.sbra, e2, diag && k2 == b ? 0.5 * sym_b : sym_b, gb, fsum);
                 w.npq += (unsigned long long)br.nprim * V.ket[k2].nprim;
             }
         } else {
             for (int t = 0; t < n; ++t) {
                 const int e2 = q[t], k2 = e2 & JK_Q_KET;
                 grad_team_quartet<C>(A, V, br, w.sbra, e2, diag && k2 == b ? 0.5 * sym_b : sym_b,
-                                     ws, lane);
+                                     ws, lane, fsum);
                 if (lane == 0) w.npq += (unsigned long long)br.nprim * V.ket[k2].nprim;
             }
         }
@@ -589,7 +598,7 @@ __device__ __forceinline__ void grad_task(const ClassArgs &A, const PlanView &V,
         double v = gb[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) atomicAdd(A.grad + (c < 3 ? ai : aj) * 3 + c % 3, v);
+        if (lane == 0) atomicAdd(fsum + (c < 3 ? ai : aj) * 3 + c % 3, v);
     }
 }
 
@@ -612,6 +621,15 @@ __global__ void __launch_bounds__(NT, 1) jk_grad_kernel(const __grid_constant__ 
     RegWarp w;
     w.sbra = smem + warp * A.max_bra_prim * JK_PRIM_STRIDE;
     double *ws = smem + NW * A.max_bra_prim * JK_PRIM_STRIDE + warp * grad_team_doubles<C>();
+    // forces: summed per block in shared memory when the atoms fit, else
+    // straight to the output
+    const bool fsmem = A.natm <= JK_GRAD_SMEM_ATOMS;
+    double *fsum = fsmem ? smem + NW * (A.max_bra_prim * JK_PRIM_STRIDE + grad_team_doubles<C>())
+                         : A.grad;
+    if (fsmem) {
+        for (int t = threadIdx.x; t < 3 * A.natm; t += NT) fsum[t] = 0.;
+        __syncthreads();
+    }
     w.sbra32 = nullptr;
     w.q = s_q[warp];
     w.staged_v = w.staged_b = -1;
@@ -620,7 +638,12 @@ __global__ void __launch_bounds__(NT, 1) jk_grad_kernel(const __grid_constant__ 
     launch_tasks(A, t_begin, t_end);
     const int chunk = *A.chunk;
     Task task;
-    while (claim_task(P, t_begin, t_end, chunk, task)) grad_task<C>(A, P.v[0], task, w, ws, lane);
+    while (claim_task(P, t_begin, t_end, chunk, task)) grad_task<C>(A, P.v[0], task, w, ws, lane, fsum);
+    if (fsmem) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < 3 * A.natm; t += NT)
+            if (fsum[t] != 0.) atomicAdd(A.grad + t, fsum[t]);
+    }
     if (lane == 0 && A.nquartets) atomicAdd(A.nquartets, w.nq);
     unsigned long long npq = w.npq;
 #pragma unroll
@@ -638,7 +661,8 @@ static int launch_grad(const ClassArgs &a, const PlanView *views, const LaunchCf
     prm.v[0] = views[0];
     auto kern = jk_grad_kernel<C, NT>;
     const size_t shm =
-        (size_t)(NT / 32) * (a.max_bra_prim * JK_PRIM_STRIDE + grad_team_doubles<C>()) * sizeof(double);
+        ((size_t)(NT / 32) * (a.max_bra_prim * JK_PRIM_STRIDE + grad_team_doubles<C>()) +
+         (a.natm <= JK_GRAD_SMEM_ATOMS ? 3 * (size_t)a.natm : 0)) * sizeof(double);
     int bps = 0;
     const int rc = configure(kern, NT, shm, ks, cfg, tag, bps);
     if (rc || cfg.configure_only) return rc;

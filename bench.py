@@ -497,8 +497,8 @@ def run_serve(args, dev):
 # DRAM (the rest hits L2), so the traffic follows the data's size, nao^2, and
 # not the quartet count; the bench scales it by (nao / 608)^2.  Source:
 # profiles/jk_class_kernels_h2o32_631gs_uhf.md.
-TRAFFIC_SMALL = {(1, 0, 0, 0): 13485056, (0, 0, 0, 0): 12207360, (1, 0, 1, 0): 13103616,
-                 (2, 0, 0, 0): 11322880, (2, 0, 1, 0): 12378368}
+TRAFFIC_SMALL = {(1, 0, 0, 0): 13473280, (0, 0, 0, 0): 12206080, (1, 0, 1, 0): 13282560,
+                 (2, 0, 0, 0): 11496448, (2, 0, 1, 0): 12419584}
 TRAFFIC_NAO = 608
 
 

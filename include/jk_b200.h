@@ -141,7 +141,10 @@ int jk_build_host(jk_plan *plan, const double *dm_host, int n_dm, int hermi,
  * a plan's first build.
  *
  * The first call on a device looks up the array's device address (with
- * that device current); make that first call before any stream capture.
+ * that device current).  The call is not capture-safe: it may wait on the
+ * plan's previous build and reuses a pinned staging buffer, so it must not
+ * be issued on a stream that is being captured into a CUDA graph (use
+ * jk_batch_* with use_graph = 1 for graph replay).
  * Every call shares the one array and it keeps the previous call's
  * contents (the accumulators are cleared at the start of each call), so
  * calls whose work overlaps on the GPU -- different streams, or different

@@ -10,7 +10,7 @@ n = 1..7 and stores the result, so that the tests can pin this project's own
 Rys roots (the oracle's and the kernels') to the reference's numbers without
 the reference being present.
 
-    python tests/golden/make_rys_golden.py [/path/to/reference]
+    python tests/golden/make_rys_golden.py /path/to/reference
 """
 import math
 import os
@@ -18,7 +18,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+if len(sys.argv) != 2:
+    sys.exit('usage: python tests/golden/make_rys_golden.py /path/to/reference')
+REF = sys.argv[1]
 TABLE = os.path.join(REF, 'electrolites', 'kernels', 'data',
                      'rys_roots_dat.npz')
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)),

@@ -23,7 +23,8 @@ EXPORTS = ['jk_plan_create', 'jk_plan_destroy', 'jk_plan_info', 'jk_build',
            'jk_plan_set_tol', 'jk_plan_set_jengine', 'jk_plan_set_tuning',
            'jk_batch_create', 'jk_batch_destroy', 'jk_batch_build', 'jk_batch_sync',
            'jk_batch_counts', 'jk_batch_set_timing', 'jk_batch_class_ms',
-           'jk_batch_set_tuning', 'jk_batch_stats', 'jk_last_error', 'jk_grad']
+           'jk_batch_set_tuning', 'jk_batch_stats', 'jk_last_error', 'jk_grad',
+           'jk_plan_set_jmd']
 
 _lib = None
 
@@ -72,6 +73,7 @@ def lib():
     L.jk_plan_set_tol.argtypes = [vp, c_double]
     L.jk_plan_set_jengine.argtypes = [vp, c_int]
     L.jk_plan_set_tuning.argtypes = [vp, c_int, c_int, c_int, c_int]
+    L.jk_plan_set_jmd.argtypes = [vp, c_int, c_int]
     L.jk_batch_create.argtypes = [c_int, ctypes.POINTER(vp)]
     L.jk_batch_destroy.argtypes = [vp]
     L.jk_batch_build.argtypes = [vp, vp, c_int, vp, vp, c_int, c_int, c_int, vp, vp, c_double,

@@ -79,6 +79,37 @@ def tune(target, run, run_mixed=None, reps: int = 2, candidates=CANDIDATES) -> d
     return table
 
 
+def tune_jmd(opt, run_j, reps: int = 2) -> dict:
+    """J-only builds: per class, the Rys J engine against the
+    McMurchie-Davidson J kernel (the reference's J engine,
+    electrolites/fastj.py:540-569, picked there per class), timed with
+    per-class CUDA events on run_j() (one synchronised J-only build on
+    opt).  Returns {class key: [rys ms, md ms, 1 if MD is kept]} for the
+    classes that have an MD kernel, and applies the choice (MD kept where it
+    is at least 3% faster)."""
+    keys = class_keys()
+    opt.set_timing(True)
+    timed = {}
+    for mode in (0, 1):
+        opt.set_jmd(mode)
+        timed[mode] = _class_ms(opt, run_j, reps)
+    opt.set_jmd(0)
+    out = {}
+    for i, k in enumerate(keys):
+        if k not in timed[1] or k not in timed[0]:
+            continue
+        try:
+            opt.set_jmd(1, i)
+        except Exception:   # noqa: BLE001 -- no MD kernel for this class
+            continue
+        rys, md = timed[0][k], timed[1][k]
+        keep = md < 0.97 * rys
+        opt.set_jmd(1 if keep else 0, i)
+        out[_key(k)] = [round(rys, 4), round(md, 4), int(keep)]
+    opt.set_timing(False)
+    return out
+
+
 def apply(target, table: dict):
     """Set a stored table on a VHFOpt or JKBatch (classes absent from the
     table keep their defaults)."""
@@ -125,6 +156,9 @@ def main():
     ap.add_argument('--out', default=TABLE_PATH)
     ap.add_argument('--reps', type=int, default=2)
     ap.add_argument('--batch-mols', type=int, default=512)
+    ap.add_argument('--jmd-only', action='store_true',
+                    help='only compare the McMurchie-Davidson J kernel with the Rys J '
+                         'engine per class (J-only builds) and print the table')
     args = ap.parse_args()
     dev = torch.device('cuda', torch.cuda.current_device())
     # single: (H2O)_96, 6-31G*, UHF pair
@@ -132,6 +166,17 @@ def main():
     dms = torch.as_tensor(clusters.uhf_pair(clusters.atomic_density(mol, 20261204), 20261205),
                           device=dev)
     opt = VHFOpt(mol, 1e-13).build()
+    if args.jmd_only:
+        for name, (m, d) in {'(H2O)96 6-31G* UHF pair': (mol, dms),
+                             '(H2O)16 def2-TZVP': (lambda m2: (m2, torch.as_tensor(
+                                 clusters.atomic_density(m2, 20261205)[None], device=dev)))(
+                                 clusters.water_mole(16, 7.8, 20261205, basis='def2-tzvp'))}.items():
+            o = opt if m is mol else VHFOpt(m, 1e-13).build()
+            t = tune_jmd(o, lambda: o.get_j(d), args.reps)
+            print(name, 'J-only, ms per class: [Rys J engine, McMurchie-Davidson, MD kept]')
+            for k, v in sorted(t.items(), key=lambda kv: -kv[1][0]):
+                print(f'  {k}  {v[0]:9.3f}  {v[1]:9.3f}  {v[2]}')
+        return
     table = tune(opt, lambda: opt.get_jk(dms, 1),
                  lambda: opt.get_jk(dms, 1, mixed_threshold=MIXED_THRESHOLD), args.reps)
     save(dev.index, 'single', table, '(H2O)96 6-31G* UHF pair', args.out)

@@ -351,6 +351,11 @@ def gen_grad_root(cls):
     return em.text()
 
 
+MD_LMAX = 6              # = JK_MD_LMAX (csrc/jk_mdj.cuh)
+# classes whose J-only builds take the McMurchie-Davidson kernel by default
+# (the per-class choice measured against the Rys J engine)
+MD_DEFAULT = frozenset()
+
 GRAD_STRAIGHT_MAX = 250   # component pairs up to which grad_root is straight-line code
 
 
@@ -517,9 +522,14 @@ def write_all(outdir, lmax=LMAX):
         # two blocks per SM ((e0|f0) block <= 27); in the larger ones the
         # second (FP32) copy of the quartet code costs more than it saves
         fp32 = 1 if cls.form == 'reg' and cls.ne * cls.nf <= 27 else 0
+        # McMurchie-Davidson J kernel (J-only builds): register-form classes
+        # up to JK_MD_LMAX; md_default: the classes where it measured faster
+        # than the Rys J engine
+        md = 1 if cls.form == 'reg' and cls.li + cls.lj + cls.lk + cls.ll <= MD_LMAX else 0
+        md_def = 1 if md and cls.tag in MD_DEFAULT else 0
         reg.append(f'    {{{A}, {B}, {cls.li}, {cls.lj}, {cls.lk}, {cls.ll}, '
                    f'{form}, {1 if cls.form == "reg" else cls.team_threads}, {fp32}, '
-                   f'jk_launch_{cls.tag}}},')
+                   f'{md}, {md_def}, jk_launch_{cls.tag}}},')
     reg.append('};')
     # J engine: pair transforms per pair class, from the (la lb|ss) units
     pairs = [(A, cls) for A, B, cls in classes if cls.lk == 0 and cls.ll == 0]

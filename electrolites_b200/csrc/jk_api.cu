@@ -129,6 +129,7 @@ struct ClassTune {
     int tasks_per_sm;    // tasks per SM the task size aims at
     int blocks_per_sm;   // cap on resident blocks per SM (0: occupancy limit)
     int fp32;            // mixed builds may run this class's low-bound quartets in FP32
+    int jmd;             // J-only builds take the McMurchie-Davidson kernel
 };
 
 // Class kernels run on this many streams: a persistent class kernel ends
@@ -179,6 +180,9 @@ struct Engine {
     // J engine of the prepared build (one plan, J only)
     int jx = 0;
     bool jx_jonly = false;          // the J engine's build has no K
+    // McMurchie-Davidson J may serve its classes: a J-only build of one plan,
+    // the Coulomb operator, at most JK_MD_DENS densities
+    bool md_ok = false;
     bool jx_reg = true;             // J/K builds: register-form classes too
     double *jx_dens = nullptr, *jx_acc = nullptr;
     const jk_plan *jx_plan = nullptr;
@@ -267,6 +271,7 @@ static void engine_defaults(Engine &E)
         E.tune[c].tasks_per_sm = jk_class_table[c].form == 0 ? 64 : 16;
         E.tune[c].blocks_per_sm = 0;
         E.tune[c].fp32 = jk_class_table[c].fp32_default;
+        E.tune[c].jmd = jk_class_table[c].md_default;
     }
 }
 
@@ -527,6 +532,7 @@ static int engine_prepare(Engine &E, std::vector<Item> &items, const Spec &s, ch
     }
     E.jx = jx;
     E.jx_jonly = !s.with_k;
+    E.md_ok = jx && !s.with_k && s.nterm == 1 && s.omega[0] == 0.0 && items[0].n_j <= JK_MD_DENS;
     E.jx_acc = jx ? (double *)(ws + o) : nullptr;
     o += jx_bytes;
     for (Item &it : items) {
@@ -787,6 +793,8 @@ static ClassArgs class_args(const Engine &E, int c, int l, int s, const PlanView
     a.jx = E.jx && (E.jx_jonly || jk_class_table[c].form == 1 || E.jx_reg)
                ? (E.jx_jonly ? 2 : 1)
                : 0;
+    // 3: McMurchie-Davidson J in place of the J engine (the class's choice)
+    if (a.jx == 2 && E.md_ok && jk_class_table[c].md && E.tune[c].jmd) a.jx = 3;
     a.jx_dens = E.jx_dens;
     a.jx_acc = E.jx_acc;
     a.grad = E.grad;
@@ -1460,6 +1468,22 @@ extern "C" int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int 
 {
     if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_tuning: plan is NULL");
     return engine_set_tuning(plan->eng, cls, tasks_per_sm, blocks_per_sm, fp32);
+}
+
+extern "C" int jk_plan_set_jmd(jk_plan *plan, int cls, int mode)
+{
+    if (!plan) return fail(JK_ERR_ARG, "jk_plan_set_jmd: plan is NULL");
+    if (cls < -1 || cls >= JK_NCLASSES) return fail(JK_ERR_ARG, "jk_plan_set_jmd: no such class");
+    if (mode < -1 || mode > 1) return fail(JK_ERR_ARG, "jk_plan_set_jmd: mode is -1, 0 or 1");
+    for (int c = cls < 0 ? 0 : cls; c < (cls < 0 ? JK_NCLASSES : cls + 1); ++c) {
+        if (mode == 1 && !jk_class_table[c].md) {
+            if (cls >= 0) return fail(JK_ERR_ARG, "jk_plan_set_jmd: the class has no MD J kernel");
+            continue;
+        }
+        plan->eng.tune[c].jmd = mode < 0 ? jk_class_table[c].md_default : mode;
+    }
+    plan->eng.tune_gen++;
+    return JK_OK;
 }
 
 // ---------------------------------------------------------------------------

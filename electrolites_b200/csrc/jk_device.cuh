@@ -47,6 +47,34 @@
 #define JK_QBIN_W 2.302585092994046f
 __host__ __device__ __forceinline__ float jk_qbin(float q) { return floorf(q / JK_QBIN_W); }
 
+// McMurchie-Davidson J (jk_mdj.cuh): densities of a build it serves (more:
+// the Rys J engine) and the largest l_i + l_j + l_k + l_l of its classes
+#define JK_MD_DENS 2
+#define JK_MD_LMAX 6
+
+// Cartesian components: count, powers and index of a level (PySCF order)
+__host__ __device__ constexpr int g_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// component d (0 x, 1 y, 2 z) of Cartesian function n of level L <= 7
+// (PySCF order: lx descending, then ly descending).  Closed form, no loop,
+// so that with constant arguments (unrolled loops) every use folds to a
+// constant and the arrays it indexes stay in registers.  k = L - lx is the
+// group of n (the groups before it hold k (k + 1) / 2 functions); within
+// it, lz = n - k (k + 1) / 2.
+__host__ __device__ constexpr int g_comp(int L, int n, int d)
+{
+    const int k = n >= 28 ? 7 : n >= 21 ? 6 : n >= 15 ? 5 : n >= 10 ? 4 : n >= 6 ? 3
+                : n >= 3 ? 2 : n >= 1 ? 1 : 0;
+    const int lz = n - k * (k + 1) / 2;
+    return d == 0 ? L - k : (d == 1 ? k - lz : lz);
+}
+
+// index of (lx, ly, lz) within its level
+__host__ __device__ constexpr int g_idx(int lx, int ly, int lz)
+{
+    return (ly + lz) * (ly + lz + 1) / 2 + lz;
+}
+
 struct PairRec {
     int ish, jsh;        // shells; ish carries the higher angular momentum
     int i0, j0;          // first Cartesian AO of each shell

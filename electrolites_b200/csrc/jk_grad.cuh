@@ -34,25 +34,6 @@
 // them to the output; larger molecules add every quartet's forces there
 #define JK_GRAD_SMEM_ATOMS 1024
 
-__host__ __device__ constexpr int g_ncart(int l) { return (l + 1) * (l + 2) / 2; }
-
-// component d (0 x, 1 y, 2 z) of Cartesian function n of level L (PySCF order)
-__host__ __device__ constexpr int g_comp(int L, int n, int d)
-{
-    int lx = L, m = n;
-    while (m >= L - lx + 1) {
-        m -= L - lx + 1;
-        --lx;
-    }
-    const int ly = L - lx - m;
-    return d == 0 ? lx : (d == 1 ? ly : L - lx - ly);
-}
-
-// index of (lx, ly, lz) within its level
-__host__ __device__ constexpr int g_idx(int lx, int ly, int lz)
-{
-    return (ly + lz) * (ly + lz + 1) / 2 + lz;
-}
 
 // derivative block X (nab x NKL, a at level la, rows (a * NB + b)) of a
 // shifted shell, contracted with W over the class's (a, b, c, d): for the

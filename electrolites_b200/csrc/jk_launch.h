@@ -24,6 +24,8 @@ struct ClassEntry {
     int form;                     // 0 register form, 1 team form
     int team_threads;
     int fp32_default;             // mixed builds run FP32 quartets here by default
+    int md;                       // a McMurchie-Davidson J kernel exists (J-only builds)
+    int md_default;               // J-only builds take it by default
     ClassLauncher launch;
 };
 

@@ -308,6 +308,12 @@ class VHFOpt:
         _lib.check(_lib.lib().jk_plan_set_shard(self.plan, int(rank), int(size)),
                    'jk_plan_set_shard')
 
+    def set_jmd(self, mode: int = 1, cls: int = -1):
+        """J-only builds: McMurchie-Davidson J kernel for class index cls
+        (-1: every class that has one) on (1), off (0) or the class's
+        default (-1)."""
+        _lib.check(_lib.lib().jk_plan_set_jmd(self.plan, int(cls), int(mode)), 'jk_plan_set_jmd')
+
     def set_tuning(self, cls: int, tasks_per_sm: int, blocks_per_sm: int = 0, fp32: int = -1):
         """Per-class launch tuning (class index k of class_keys(); -1 resets
         every class)."""

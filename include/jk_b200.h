@@ -277,6 +277,18 @@ int jk_plan_set_tuning(jk_plan *plan, int cls, int tasks_per_sm, int blocks_per_
                        int fp32);
 
 /*
+ * J-only builds: which classes take the McMurchie-Davidson J kernel in place
+ * of the Rys J engine -- the reference's J engine
+ * (electrolites/fastj.py:540-569, per-class kernels j_<lij>_<lkl>), here a
+ * register-form kernel per class up to l_i + l_j + l_k + l_l = 6, chosen per
+ * class by measurement.  mode 1: on, 0: off, -1: the class's default; cls =
+ * -1: every class that has the kernel.  It serves builds of the Coulomb
+ * operator with up to two densities; others keep the Rys J engine.
+ * JK_ERR_ARG for a class without the kernel.
+ */
+int jk_plan_set_jmd(jk_plan *plan, int cls, int mode);
+
+/*
  * Batched builds: J/K for many molecules (plans) in one launch stream, each
  * with its own densities (n_dm[i] of them, dms[i] on the device) and
  * outputs (vj[i], vk[i]).  Each angular-momentum class runs as one

@@ -83,3 +83,37 @@ def test_committed_table_is_well_formed():
             for key, v in entry.get(form, {}).items():
                 assert len(key) == 4 and key.isdigit()
                 assert v[0] > 0 and v[1] >= 0 and (len(v) < 3 or v[2] in (-1, 0, 1))
+
+
+class FakeJmd:
+    """J-only per-class times: class 0 is faster with the MD kernel, class 1
+    slower, class 2 has no MD kernel (set_jmd on it raises)."""
+
+    def __init__(self, keys):
+        self.keys = keys
+        self.mode = {i: 0 for i in range(len(keys))}
+
+    def set_timing(self, on=True):
+        pass
+
+    def set_jmd(self, mode=1, cls=-1):
+        if cls == 2 and mode == 1:
+            raise RuntimeError('no MD kernel')
+        for i in (range(len(self.keys)) if cls < 0 else [cls]):
+            if i != 2:
+                self.mode[i] = mode
+
+    def last_class_ms(self):
+        base = {0: 10.0, 1: 10.0, 2: 5.0}
+        md = {0: 8.0, 1: 14.0, 2: 5.0}
+        return {k: (md[i] if self.mode[i] else base[i]) for i, k in enumerate(self.keys)}, 1
+
+
+def test_tune_jmd_keeps_md_where_faster(monkeypatch):
+    from electrolites_b200 import autotune
+    keys = [(1, 0, 0, 0), (2, 0, 0, 0), (3, 3, 3, 3)]
+    monkeypatch.setattr(autotune, 'class_keys', lambda: keys)
+    t = FakeJmd(keys)
+    out = autotune.tune_jmd(t, lambda: None, reps=1)
+    assert out == {'1000': [10.0, 8.0, 1], '2000': [10.0, 14.0, 0]}
+    assert t.mode == {0: 1, 1: 0, 2: 0}

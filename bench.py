@@ -391,6 +391,65 @@ def run_rsh(args, dev, stream, flush, opt, dms):
             'max_dK': float((vk - ka - kb).abs().max())}
 
 
+def run_jonly(args, dev, stream, flush, opt, dms):
+    """J-only builds of the main workload (the reference's get_j): the
+    default per-class choice (the Rys J engine where it measured faster)
+    against the McMurchie-Davidson kernel in every class that has one;
+    device ms per build and the largest element difference."""
+    import torch
+    vj = torch.empty_like(dms)
+    opt.set_jmd(-1)
+    dflt = _timed(lambda: opt.build_jk_async(dms, 1, True, False, vj, None, 0.0, stream),
+                  2, 1, stream, flush)
+    opt.sync(stream)
+    ref = vj.clone()
+    opt.set_jmd(1)
+    md = _timed(lambda: opt.build_jk_async(dms, 1, True, False, vj, None, 0.0, stream),
+                2, 1, stream, flush)
+    opt.sync(stream)
+    opt.set_jmd(-1)
+    return {'default_ms': round(dflt, 2), 'md_every_class_ms': round(md, 2),
+            'max_dJ': float((vj - ref).abs().max())}
+
+
+GRAD_WORKLOAD, GRAD_CHECK = 'h2o32_631gs_uhf', 'h2o8_631gs'
+GRAD_J, GRAD_K = 1.0, 0.2
+
+
+def run_grad(args, dev, stream, flush, check):
+    """Nuclear gradient of the two-electron energy (the reference's
+    fastejk, jk_grad): device ms per gradient on (H2O)_32 6-31G* UHF against
+    one J/K build of the same densities, and (check) the gradient of the
+    (H2O)_8 UHF pair against the checker's analytic gradient."""
+    import numpy as np
+    import torch
+
+    from electrolites_b200 import clusters
+    from electrolites_b200.jk import VHFOpt
+    mol, dms_h = make_inputs(GRAD_WORKLOAD)
+    opt = VHFOpt(mol, TOL).build()
+    dms = torch.as_tensor(dms_h, device=dev)
+    g_ms = _timed(lambda: opt.jk_energy_per_atom(dms, GRAD_J, GRAD_K, stream=stream), 2, 1,
+                  stream, flush)
+    jk_ms = _timed(lambda: opt.build_jk_async(dms, 1, stream=stream), 2, 1, stream, flush)
+    opt.sync(stream)
+    out = {'workload': GRAD_WORKLOAD, 'j_factor': GRAD_J, 'k_factor': GRAD_K,
+           'natm': int(mol.natm), 'grad_ms': round(g_ms, 2), 'jk_build_ms': round(jk_ms, 2),
+           'ratio': round(g_ms / jk_ms, 2)}
+    if check:
+        from oracle import oracle as O
+        mc, dc = make_inputs(GRAD_CHECK)
+        dc = clusters.uhf_pair(dc[0], 20261208)
+        oc = VHFOpt(mc, TOL).build()
+        g = oc.jk_energy_per_atom(torch.as_tensor(dc, device=dev), GRAD_J, GRAD_K).cpu().numpy()
+        rg, _ = O.grad_jk_fast(mc, dc, GRAD_J, GRAD_K, tol=TOL, nthreads=host_cores())
+        err = float(np.abs(g - rg).max() / np.abs(rg).max())
+        out['check'] = {'workload': GRAD_CHECK + ' UHF pair', 'max_rel_err': err,
+                        'force_sum': float(np.abs(g.sum(axis=0)).max()),
+                        'checker': 'oracle/jk_check.c', 'pass': err <= 1e-9}
+    return out
+
+
 SCF_CYCLES, SCF_SIGMA0, SCF_DECAY, SCF_SEED = 14, 3e-2, 0.5, 20261207
 
 
@@ -652,6 +711,8 @@ def run_ours(args, rank, world):
         bg.start()
 
     rsh = run_rsh(args, dev, stream, flush, opt, dms) if solo and not args.no_rsh else None
+    jonly = run_jonly(args, dev, stream, flush, opt, dms) if solo and not args.no_jonly else None
+    grad = run_grad(args, dev, stream, flush, check) if solo and not args.no_grad else None
     scf_screen = (run_scf_screen(args, dev, stream, opt, dms_h)
                   if solo and not args.no_scf_screen else None)
     mixed = mixed_host = None
@@ -731,6 +792,8 @@ def run_ours(args, rank, world):
             'cpu_baseline': cpu,
             'mixed': mixed,
             'range_separated': rsh,
+            'j_only': jonly,
+            'gradient': grad,
             'loose_then_tight': scf_screen,
             'batched': batched,
             'serving': serving,
@@ -810,6 +873,10 @@ def main():
                     help='skip the loose-then-tight screening trajectory')
     ap.add_argument('--no-rsh', action='store_true',
                     help='skip the fused range-separated exchange comparison')
+    ap.add_argument('--no-jonly', action='store_true',
+                    help='skip the J-only builds (Rys J engine against McMurchie-Davidson)')
+    ap.add_argument('--no-grad', action='store_true',
+                    help='skip the nuclear-gradient measurement')
     ap.add_argument('--no-batch', action='store_true',
                     help='skip the uneven-batch comparison (plain vs batched vs mixed)')
     ap.add_argument('--dry-run', action='store_true',

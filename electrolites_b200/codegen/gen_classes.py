@@ -356,7 +356,12 @@ MD_LMAX = 6              # = JK_MD_LMAX (csrc/jk_mdj.cuh)
 # (the per-class choice measured against the Rys J engine)
 MD_DEFAULT = frozenset()
 
-GRAD_STRAIGHT_MAX = 250   # component pairs up to which grad_root is straight-line code
+# component pairs up to which grad_root is straight-line code and the class
+# takes the per-lane gradient kernel: measured on (H2O)_32 6-31G* UHF, the
+# per-lane form beats the per-warp one up to (dp|ds) (421 pairs; (pp|pp)
+# 19.5 -> 10.8 ms, (dd|ps) 17.2 -> 11.2 ms) and loses at (dp|pp) (485: 16.1
+# -> 19.2 ms)
+GRAD_STRAIGHT_MAX = 450
 
 
 def grad_members(cls):

@@ -199,3 +199,38 @@ def test_module_plan_cache_follows_the_geometry():
     assert _opt_key(mol) != k0
     mol._env[ptr] -= 0.1
     assert _opt_key(mol) == k0
+
+
+def test_patched_gradient_target(monkeypatch):
+    """The patched grad.rhf._jk_energy_per_atom brings the density to the
+    option's sorted Cartesian basis through the option object and takes the
+    operator's omega from the option's molecule (the reference's fastejk,
+    electrolites/fastejk.py:270-276)."""
+    import numpy as np
+
+    import electrolites_b200 as eb
+    seen = []
+
+    class G:
+        def cpu(self):
+            return self
+
+        def numpy(self):
+            return np.zeros((2, 3))
+
+    class Plan:
+        def jk_energy_per_atom(self, dms, j, k, omega):
+            seen.append((dms, j, k, omega))
+            return G()
+
+    class Opt:
+        def apply_coeff_C_mat_CT(self, dm):
+            return ('cart', dm.shape)
+
+    opt = Opt()
+    opt.mol = types.SimpleNamespace(nao=3, omega=-0.25)
+    opt._jk_b200 = Plan()
+    out = eb._jk_energy_per_atom(opt, np.zeros((2, 3, 3)), 1.0, 0.3)
+    assert out.shape == (2, 3)
+    assert seen == [(('cart', (2, 3, 3)), 1.0, 0.3, -0.25)]
+

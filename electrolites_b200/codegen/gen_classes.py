@@ -523,10 +523,11 @@ def write_all(outdir, lmax=LMAX):
     reg.append('static const ClassEntry jk_class_table[JK_NCLASSES] = {')
     for A, B, cls in classes:
         form = 0 if cls.form == 'reg' else 1
-        # FP32 quartets by default only in the register-form classes that run
-        # two blocks per SM ((e0|f0) block <= 27); in the larger ones the
-        # second (FP32) copy of the quartet code costs more than it saves
-        fp32 = 1 if cls.form == 'reg' and cls.ne * cls.nf <= 27 else 0
+        # FP32 quartets by default in the register-form classes that run two
+        # blocks per SM ((e0|f0) block <= 27; in the larger register-form
+        # ones the second (FP32) copy of the quartet code costs more than it
+        # saves) and in the team form (FP32 2D integrals in shared memory)
+        fp32 = 1 if (cls.form == 'reg' and cls.ne * cls.nf <= 27) or cls.form != 'reg' else 0
         # McMurchie-Davidson J kernel (J-only builds): register-form classes
         # up to JK_MD_LMAX; md_default: the classes where it measured faster
         # than the Rys J engine

@@ -402,3 +402,34 @@ def test_parity_at_bench_sizes(torch, oracle, name):
     ej, ek = _energies(dms, gj, gk)
     rej, rek = _energies(dms, rj, rk)
     assert abs(ej - rej) <= ETOL and abs(ek - rek) <= ETOL, (ej - rej, ek - rek)
+
+
+@pytest.mark.parametrize('seed', [34, 35])
+def test_mixed_form_team_classes(torch, oracle, seed):
+    """FP32 quartets of the mixed form in the team-form classes (the f-shell
+    and (dd|ds)-and-larger classes), on a spread-out (H2O)_4 def2-TZVP
+    cluster whose distant quartets fall below the threshold: at 1e-6 some
+    team-class quartets run in FP32 and the J/K energies stay within 1e-7 Eh
+    of the checker's; with the threshold off no quartet runs in FP32."""
+    import ctypes
+
+    from electrolites_b200 import _lib
+    from electrolites_b200.jk import VHFOpt, class_keys
+    mol = clusters.water_mole(4, 8.0, seed, basis='def2-tzvp')
+    dms = clusters.uhf_pair(clusters.atomic_density(mol, seed), seed + 1)
+    opt = VHFOpt(mol, TOL).build()
+    d = torch.as_tensor(dms, device='cuda')
+    forms = {}
+    for k in range(len(class_keys())):
+        ls = [ctypes.c_int() for _ in range(5)]
+        _lib.lib().jk_class_info(k, *[ctypes.byref(x) for x in ls])
+        forms[tuple(x.value for x in ls[:4])] = ls[4].value
+    mj, mk = opt.get_jk(d, 1, mixed_threshold=1e-6)
+    counts = opt.class_counts(with_f32=True)
+    assert sum(c[2] for k, c in counts.items() if forms[k] == 1) > 0
+    rj, rk, _ = oracle.jk_fast(mol, dms, tol=TOL)
+    ej, ek = _energies(dms, rj, rk)
+    mej, mek = _energies(dms, mj.cpu().numpy(), mk.cpu().numpy())
+    assert abs(ej - mej) <= 1e-7 and abs(ek - mek) <= 1e-7
+    opt.get_jk(d, 1)
+    assert sum(c[2] for c in opt.class_counts(with_f32=True).values()) == 0

@@ -305,15 +305,22 @@ def _level_set(l0, l1):
     return [(L, c) for L in range(l0, l1 + 1) for c in comps(L)]
 
 
-def gen_grad_root(cls):
+def gen_grad_root(cls, only=None):
     """One Rys root's contribution to the four gradient blocks:
-    R[fi * NE_R + ei] (+)= w * G_x G_y G_z over the block's components."""
+    R[fi * NE_R + ei] (+)= w * G_x G_y G_z over the block's components.
+    only: one block's name -- that block alone, written to R with weight w
+    (the split classes accumulate one block per pass)."""
     em = Emitter('    ')
     lij1, lkl1 = cls.lij + 1, cls.lkl + 1
+    rects = grad_rects(cls)
+    if only is not None:
+        rects = [('R', e, f, None if w is None else 'w') for name, e, f, w in rects if name == only]
+        # the recurrences only as far as this block reads them
+        lij1 = max(e[1] for _, e, _, _ in rects)
+        lkl1 = max(f[1] for _, _, f, _ in rects)
     gx = gen_vrr(em, cls, 'x', '1', lij1, lkl1)
     gy = gen_vrr(em, cls, 'y', '1', lij1, lkl1)
     gz = gen_vrr(em, cls, 'z', 'wz', lij1, lkl1)
-    rects = grad_rects(cls)
     # every (e, f) component pair of any block, once
     members = {}
     for name, (e0, e1), (f0, f1), w in rects:
@@ -362,6 +369,14 @@ MD_DEFAULT = frozenset()
 # 19.5 -> 10.8 ms, (dd|ps) 17.2 -> 11.2 ms) and loses at (dp|pp) (485: 16.1
 # -> 19.2 ms)
 GRAD_STRAIGHT_MAX = 450
+# per-lane classes with more block products than this accumulate one block
+# per pass over the primitives (recurrences and roots recomputed per pass):
+# with all four blocks live the accumulators spill to local memory, and the
+# (dp|ps) kernel moved 56 GB through DRAM per launch on (H2O)_32 6-31G* UHF.
+# Measured there: split, (pp|pp) 10.8 -> 6.2 ms, (ds|pp) 18.4 -> 14.5, (dp|ps)
+# 17.1 -> 14.6, (dd|ps) 11.2 -> 9.2; but (ds|ps) (102 products) 10.0 -> 19.8
+# and (pp|ps) (124) 9.5 -> 13.3, which stay single-pass
+GRAD_SPLIT_MIN = 150
 
 
 def grad_members(cls):
@@ -384,7 +399,9 @@ def gen_grad_struct(cls):
     lines = []
     rects = grad_rects(cls)
     small = len(grad_members(cls)) <= GRAD_STRAIGHT_MAX
+    split = small and len(grad_members(cls)) > GRAD_SPLIT_MIN
     lines.append(f'    static constexpr bool G_SMALL = {"true" if small else "false"};')
+    lines.append(f'    static constexpr bool G_SPLIT = {"true" if split else "false"};')
     for name, (e0, e1), (f0, f1), _ in rects:
         ne = len(_level_set(e0, e1))
         nf = len(_level_set(f0, f1))
@@ -399,11 +416,17 @@ def gen_grad_struct(cls):
     lines.append(f'    static constexpr int G_U_E_LI = {off(ue0, li)};    // level li in U\'s e range')
     lines.append(f'    static constexpr int G_U_F_LK = {off(uf0, lk)};    // level lk in U\'s f range')
     tpl = 'template <class T> __device__ static __forceinline__ void'
-    if small:
+    if small and not split:
         lines.append(f'    {tpl} grad_root(T c0x, T c0y, T c0z, T cpx, T cpy, T cpz, T b00, '
                      'T b10, T b01, T wz, T wA, T wB, T wC, T *U, T *RA, T *RB, T *RC) {')
         lines.append(gen_grad_root(cls))
         lines.append('    }')
+    if split:
+        for name, _, _, _ in rects:
+            lines.append(f'    {tpl} grad_root_{name}(T c0x, T c0y, T c0z, T cpx, T cpy, T cpz, '
+                         'T b00, T b10, T b01, T wz, T w, T *R) {')
+            lines.append(gen_grad_root(cls, only=name))
+            lines.append('    }')
     tpl_s = ('template <class T, int SI = 1, int SO = 1> __device__ static __forceinline__ '
              'void')
     shifts = [('ip', li + 1, lj, 'hbi', 'AB'), ('jp', li, lj + 1, 'hbj', 'AB'),

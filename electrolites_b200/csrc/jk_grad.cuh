@@ -117,27 +117,17 @@ __device__ __forceinline__ void grad_bra_block(const double *R, int ne, HB hb,
     }
 }
 
-template <class C>
-__device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView &V,
-                                             const PairRec &br, const double *__restrict__ sbra,
-                                             int entry, double sym, double gb[6], double *fsum)
+// The primitive loop of one quartet: per primitive quartet and Rys root the
+// generated root routine adds to the blocks.  R = -1: all four blocks at once
+// (grad_root); R = 0..3: U, RA, RB or RC alone (the split classes'
+// grad_root_U .. grad_root_RC; the other pointers are unused).
+template <class C, int R>
+__device__ __forceinline__ void grad_accum(const ClassArgs &A, const PlanView &V,
+                                           const PairRec &br, const PairRec &kt,
+                                           const double *__restrict__ sbra, double *U, double *RA,
+                                           double *RB, double *RC)
 {
-        constexpr int LI = C::LI, LJ = C::LJ, LK = C::LK, LL = C::LL;
-    constexpr int NI = C::NI, NJ = C::NJ, NK = C::NK, NL = C::NL;
-    constexpr int NIJ = NI * NJ, NKL = NK * NL;
     constexpr int NR = C::G_NROOTS;
-    const int kk = entry & JK_Q_KET;
-    const PairRec kt = V.ket[kk];
-    double U[C::G_U_NE * C::G_U_NF], RA[C::G_RA_NE * C::G_RA_NF];
-    double RB[C::G_RB_NE * C::G_RB_NF], RC[C::G_RC_NE * C::G_RC_NF];
-#pragma unroll
-    for (int n = 0; n < C::G_U_NE * C::G_U_NF; ++n) U[n] = 0.;
-#pragma unroll
-    for (int n = 0; n < C::G_RA_NE * C::G_RA_NF; ++n) RA[n] = 0.;
-#pragma unroll
-    for (int n = 0; n < C::G_RB_NE * C::G_RB_NF; ++n) RB[n] = 0.;
-#pragma unroll
-    for (int n = 0; n < C::G_RC_NE * C::G_RC_NF; ++n) RC[n] = 0.;
     const double io2 = A.op_inv_om2[0];
     const double *cheb = A.rys + rys_offset<NR>();
     for (int kp = 0; kp < kt.nprim; ++kp) {
@@ -166,16 +156,36 @@ __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView 
                 const double c0z = fma(-up, PQz, PAz), cpx = fma(uq, PQx, QCx);
                 const double cpy = fma(uq, PQy, QCy), cpz = fma(uq, PQz, QCz);
                 const double b10 = fma(-hip, up, hip), b01 = fma(-hiq, uq, hiq);
-                C::template grad_root<double>(c0x, c0y, c0z, cpx, cpy, cpz, 0.5 * uis, b10, b01,
-                                              w[n] * pref, wA, wB, wC, U, RA, RB, RC);
+                const double wz = w[n] * pref, b00 = 0.5 * uis;
+                if constexpr (R < 0)
+                    C::template grad_root<double>(c0x, c0y, c0z, cpx, cpy, cpz, b00, b10, b01, wz,
+                                                  wA, wB, wC, U, RA, RB, RC);
+                else if constexpr (R == 0)
+                    C::template grad_root_U<double>(c0x, c0y, c0z, cpx, cpy, cpz, b00, b10, b01, wz,
+                                                    1.0, U);
+                else if constexpr (R == 1)
+                    C::template grad_root_RA<double>(c0x, c0y, c0z, cpx, cpy, cpz, b00, b10, b01, wz,
+                                                     wA, RA);
+                else if constexpr (R == 2)
+                    C::template grad_root_RB<double>(c0x, c0y, c0z, cpx, cpy, cpz, b00, b10, b01, wz,
+                                                     wB, RB);
+                else
+                    C::template grad_root_RC<double>(c0x, c0y, c0z, cpx, cpy, cpz, b00, b10, b01, wz,
+                                                     wC, RC);
             }
         }
     }
-    const double fac = kt.ish == kt.jsh ? 0.5 * sym : sym;
-    // W = fac [wj Dt_ab Dt_cd - wk sum_s (D_ac D_bd + D_ad D_bc)], Dt = (D + D^T)/2 summed
+}
+
+// W = fac [wj Dt_ab Dt_cd - wk sum_s (D_ac D_bd + D_ad D_bc)], Dt = (D + D^T)/2 summed
+template <class C>
+__device__ __forceinline__ void grad_w(const ClassArgs &A, const PlanView &V, const PairRec &br,
+                                       const PairRec &kt, double fac, double *Wt)
+{
+    constexpr int NI = C::NI, NJ = C::NJ, NK = C::NK, NL = C::NL;
+    constexpr int NIJ = NI * NJ, NKL = NK * NL;
     const size_t nao = V.nao, nao2 = nao * nao;
     const int i0 = br.i0, j0 = br.j0, k0 = kt.i0, l0 = kt.j0;
-    double Wt[NIJ * NKL];
     {
         double dab[NIJ], dcd[NKL];
 #pragma unroll
@@ -230,17 +240,17 @@ __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView 
                         Wt[((a * NJ + b) * NK + c) * NL + e] -=
                             wk * fma(dac[a * NK + c], dbd[b * NL + e], dad[a * NL + e] * dbc[b * NK + c]);
     }
-    double gA[3] = {0., 0., 0.}, gB[3] = {0., 0., 0.}, gC[3] = {0., 0., 0.};
-    // shell i raised (RA) and lowered (U from level li - 1)
-    {
-        constexpr int NAB = g_ncart(LI + 1) * NJ;
-        double X[NAB * NKL];
-        grad_bra_block<C, NAB>(RA, C::G_RA_NE,
-                               [](const double *in, double *out, double x, double y, double z) {
-                                   C::template hrr_ip<double>(in, out, x, y, z);
-                               }, br, kt, X);
-        grad_bra_contract<C, 0, LI + 1, 1>(X, Wt, gA);
-    }
+}
+
+// the derivative contributions of each block, contracted with W
+// U: shells i, j and k lowered
+template <class C>
+__device__ __forceinline__ void grad_from_u(const double *U, const double *Wt, const PairRec &br,
+                                            const PairRec &kt, double gA[3], double gB[3],
+                                            double gC[3])
+{
+    constexpr int LI = C::LI, LJ = C::LJ, LK = C::LK, LL = C::LL;
+    constexpr int NI = C::NI, NJ = C::NJ, NL = C::NL, NIJ = NI * NJ, NKL = C::NK * NL;
     if constexpr (LI > 0) {
         constexpr int NAB = g_ncart(LI - 1) * NJ;
         double X[NAB * NKL];
@@ -250,16 +260,6 @@ __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView 
                                }, br, kt, X);
         grad_bra_contract<C, 0, LI - 1, -1>(X, Wt, gA);
     }
-    // shell j raised (RB) and lowered (U from level li)
-    {
-        constexpr int NAB = NI * g_ncart(LJ + 1);
-        double X[NAB * NKL];
-        grad_bra_block<C, NAB>(RB, C::G_RB_NE,
-                               [](const double *in, double *out, double x, double y, double z) {
-                                   C::template hrr_jp<double>(in, out, x, y, z);
-                               }, br, kt, X);
-        grad_bra_contract<C, 1, LJ + 1, 1>(X, Wt, gB);
-    }
     if constexpr (LJ > 0) {
         constexpr int NAB = NI * g_ncart(LJ - 1);
         double X[NAB * NKL];
@@ -268,23 +268,6 @@ __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView 
                                    C::template hrr_jm<double>(in, out, x, y, z);
                                }, br, kt, X);
         grad_bra_contract<C, 1, LJ - 1, -1>(X, Wt, gB);
-    }
-    // shell k raised (RC: f levels lk+1 ..) and lowered (U: f levels lk-1 ..)
-    {
-        constexpr int NFS = C::G_RC_NF, NKS = g_ncart(LK + 1) * NL;
-        double tb[NFS * NIJ];
-#pragma unroll
-        for (int f = 0; f < NFS; ++f)
-            C::template hrr_bra<double>(RC + f * C::G_RC_NE, tb + f * NIJ, br.ABx, br.ABy, br.ABz);
-        double X[NIJ * NKS];
-#pragma unroll
-        for (int ij = 0; ij < NIJ; ++ij) {
-            double row[NFS];
-#pragma unroll
-            for (int f = 0; f < NFS; ++f) row[f] = tb[f * NIJ + ij];
-            C::template hrr_kp<double>(row, X + ij * NKS, kt.ABx, kt.ABy, kt.ABz);
-        }
-        grad_ket_contract<C, LK + 1, 1>(X, Wt, gC);
     }
     if constexpr (LK > 0) {
         // U's f range is [lk - 1, lkl]; the lowered transfer reads [lk - 1, lkl - 1]
@@ -303,6 +286,128 @@ __device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView 
             C::template hrr_km<double>(row, X + ij * NKS, kt.ABx, kt.ABy, kt.ABz);
         }
         grad_ket_contract<C, LK - 1, -1>(X, Wt, gC);
+    }
+}
+
+// RA: shell i raised
+template <class C>
+__device__ __forceinline__ void grad_from_ra(const double *RA, const double *Wt, const PairRec &br,
+                                             const PairRec &kt, double gA[3])
+{
+    constexpr int NAB = g_ncart(C::LI + 1) * C::NJ, NKL = C::NK * C::NL;
+    double X[NAB * NKL];
+    grad_bra_block<C, NAB>(RA, C::G_RA_NE,
+                           [](const double *in, double *out, double x, double y, double z) {
+                               C::template hrr_ip<double>(in, out, x, y, z);
+                           }, br, kt, X);
+    grad_bra_contract<C, 0, C::LI + 1, 1>(X, Wt, gA);
+}
+
+// RB: shell j raised
+template <class C>
+__device__ __forceinline__ void grad_from_rb(const double *RB, const double *Wt, const PairRec &br,
+                                             const PairRec &kt, double gB[3])
+{
+    constexpr int NAB = C::NI * g_ncart(C::LJ + 1), NKL = C::NK * C::NL;
+    double X[NAB * NKL];
+    grad_bra_block<C, NAB>(RB, C::G_RB_NE,
+                           [](const double *in, double *out, double x, double y, double z) {
+                               C::template hrr_jp<double>(in, out, x, y, z);
+                           }, br, kt, X);
+    grad_bra_contract<C, 1, C::LJ + 1, 1>(X, Wt, gB);
+}
+
+// RC: shell k raised (f levels lk + 1 ..)
+template <class C>
+__device__ __forceinline__ void grad_from_rc(const double *RC, const double *Wt, const PairRec &br,
+                                             const PairRec &kt, double gC[3])
+{
+    constexpr int NIJ = C::NI * C::NJ;
+    constexpr int NFS = C::G_RC_NF, NKS = g_ncart(C::LK + 1) * C::NL;
+    double tb[NFS * NIJ];
+#pragma unroll
+    for (int f = 0; f < NFS; ++f)
+        C::template hrr_bra<double>(RC + f * C::G_RC_NE, tb + f * NIJ, br.ABx, br.ABy, br.ABz);
+    double X[NIJ * NKS];
+#pragma unroll
+    for (int ij = 0; ij < NIJ; ++ij) {
+        double row[NFS];
+#pragma unroll
+        for (int f = 0; f < NFS; ++f) row[f] = tb[f * NIJ + ij];
+        C::template hrr_kp<double>(row, X + ij * NKS, kt.ABx, kt.ABy, kt.ABz);
+    }
+    grad_ket_contract<C, C::LK + 1, 1>(X, Wt, gC);
+}
+
+template <class C>
+__device__ __forceinline__ void grad_quartet(const ClassArgs &A, const PlanView &V,
+                                             const PairRec &br, const double *__restrict__ sbra,
+                                             int entry, double sym, double gb[6], double *fsum)
+{
+    constexpr int NIJ = C::NI * C::NJ, NKL = C::NK * C::NL;
+    constexpr int NU = C::G_U_NE * C::G_U_NF, NRA = C::G_RA_NE * C::G_RA_NF;
+    constexpr int NRB = C::G_RB_NE * C::G_RB_NF, NRC = C::G_RC_NE * C::G_RC_NF;
+    const int kk = entry & JK_Q_KET;
+    const PairRec kt = V.ket[kk];
+    const double fac = kt.ish == kt.jsh ? 0.5 * sym : sym;
+    double gA[3] = {0., 0., 0.}, gB[3] = {0., 0., 0.}, gC[3] = {0., 0., 0.};
+    if constexpr (!C::G_SPLIT) {
+        double U[NU], RA[NRA], RB[NRB], RC[NRC];
+#pragma unroll
+        for (int n = 0; n < NU; ++n) U[n] = 0.;
+#pragma unroll
+        for (int n = 0; n < NRA; ++n) RA[n] = 0.;
+#pragma unroll
+        for (int n = 0; n < NRB; ++n) RB[n] = 0.;
+#pragma unroll
+        for (int n = 0; n < NRC; ++n) RC[n] = 0.;
+        grad_accum<C, -1>(A, V, br, kt, sbra, U, RA, RB, RC);
+        double Wt[NIJ * NKL];
+        grad_w<C>(A, V, br, kt, fac, Wt);
+        grad_from_ra<C>(RA, Wt, br, kt, gA);
+        grad_from_rb<C>(RB, Wt, br, kt, gB);
+        grad_from_rc<C>(RC, Wt, br, kt, gC);
+        grad_from_u<C>(U, Wt, br, kt, gA, gB, gC);
+    } else {
+        // one block per pass over the primitives; W re-formed for each
+        // contraction (density loads, L1/L2 hits) rather than kept live
+        // through the primitive loops
+        {
+            double U[NU];
+#pragma unroll
+            for (int n = 0; n < NU; ++n) U[n] = 0.;
+            grad_accum<C, 0>(A, V, br, kt, sbra, U, nullptr, nullptr, nullptr);
+            double Wt[NIJ * NKL];
+            grad_w<C>(A, V, br, kt, fac, Wt);
+            grad_from_u<C>(U, Wt, br, kt, gA, gB, gC);
+        }
+        {
+            double RA[NRA];
+#pragma unroll
+            for (int n = 0; n < NRA; ++n) RA[n] = 0.;
+            grad_accum<C, 1>(A, V, br, kt, sbra, nullptr, RA, nullptr, nullptr);
+            double Wt[NIJ * NKL];
+            grad_w<C>(A, V, br, kt, fac, Wt);
+            grad_from_ra<C>(RA, Wt, br, kt, gA);
+        }
+        {
+            double RB[NRB];
+#pragma unroll
+            for (int n = 0; n < NRB; ++n) RB[n] = 0.;
+            grad_accum<C, 2>(A, V, br, kt, sbra, nullptr, nullptr, RB, nullptr);
+            double Wt[NIJ * NKL];
+            grad_w<C>(A, V, br, kt, fac, Wt);
+            grad_from_rb<C>(RB, Wt, br, kt, gB);
+        }
+        {
+            double RC[NRC];
+#pragma unroll
+            for (int n = 0; n < NRC; ++n) RC[n] = 0.;
+            grad_accum<C, 3>(A, V, br, kt, sbra, nullptr, nullptr, nullptr, RC);
+            double Wt[NIJ * NKL];
+            grad_w<C>(A, V, br, kt, fac, Wt);
+            grad_from_rc<C>(RC, Wt, br, kt, gC);
+        }
     }
 #pragma unroll
     for (int x = 0; x < 3; ++x) {

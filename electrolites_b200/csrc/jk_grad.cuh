@@ -438,7 +438,9 @@ struct GradTeam {
     static constexpr int NR = C::G_NROOTS;
     static constexpr int NIJKL = C::NI * C::NJ * C::NK * C::NL;
     static constexpr int SK = LL + 1, SJ = (LK + 2) * SK, SI = (LJ + 2) * SJ;
-    static constexpr int GS = (LI + 2) * SI;                 // one root and direction
+    // one root and direction, padded to an odd count so that the 3 NR lanes
+    // writing their tables at the same offsets hit different banks
+    static constexpr int GS = ((LI + 2) * SI) | 1;
     static constexpr int W = 0, RW = NIJKL, G = (RW + 2 * NR + 1) & ~1;
     static constexpr int SIZE = G + 3 * NR * GS;             // doubles per warp
     // warps per block: as many as fit in about 150 KB beside the bra records
@@ -451,7 +453,7 @@ struct GradTeam {
 // level by level in place and, for each (i, j) row kept, the ket transfer the
 // same way; out[((i * (lj + 2) + j) * (lk + 2) + k) * (ll + 1) + l]
 template <class C>
-__device__ __noinline__ void grad_team_table(double c0, double cp, double b00, double b10, double b01,
+__device__ __forceinline__ void grad_team_table(double c0, double cp, double b00, double b10, double b01,
                                              double g00, double ab, double cd, double *out)
 {
     using T = GradTeam<C>;
@@ -459,41 +461,41 @@ __device__ __noinline__ void grad_team_table(double c0, double cp, double b00, d
     double v[(E1 + 1) * FW];
     v[0] = g00;
     v[FW] = c0 * g00;
-#pragma unroll 1
+#pragma unroll
     for (int e = 1; e < E1; ++e) v[(e + 1) * FW] = fma(e * b10, v[(e - 1) * FW], c0 * v[e * FW]);
-#pragma unroll 1
+#pragma unroll
     for (int f = 0; f < F1; ++f) {
         v[f + 1] = f ? fma(f * b01, v[f - 1], cp * v[f]) : cp * v[f];
-#pragma unroll 1
+#pragma unroll
         for (int e = 1; e <= E1; ++e) {
             double t = fma(e * b00, v[(e - 1) * FW + f], cp * v[e * FW + f]);
             if (f) t = fma(f * b01, v[e * FW + f - 1], t);
             v[e * FW + f + 1] = t;
         }
     }
-#pragma unroll 1
+#pragma unroll
     for (int j = 0; j <= T::LJ + 1; ++j) {
         if (j) {   // level j from level j - 1: rows i <= E1 - j
-#pragma unroll 1
+#pragma unroll
             for (int i = 0; i <= E1 - j; ++i)
-#pragma unroll 1
+#pragma unroll
                 for (int f = 0; f < FW; ++f) v[i * FW + f] = fma(ab, v[i * FW + f], v[(i + 1) * FW + f]);
         }
         const int imax = T::LI + 1 < E1 - j ? T::LI + 1 : E1 - j;
-#pragma unroll 1
+#pragma unroll
         for (int i = 0; i <= imax; ++i) {
             double r[FW];
-#pragma unroll 1
+#pragma unroll
             for (int f = 0; f < FW; ++f) r[f] = v[i * FW + f];
             double *o = out + i * T::SI + j * T::SJ;
-#pragma unroll 1
+#pragma unroll
             for (int l = 0; l <= T::LL; ++l) {
                 if (l) {
-#pragma unroll 1
+#pragma unroll
                     for (int k = 0; k <= F1 - l; ++k) r[k] = fma(cd, r[k], r[k + 1]);
                 }
                 const int kmax = T::LK + 1 < F1 - l ? T::LK + 1 : F1 - l;
-#pragma unroll 1
+#pragma unroll
                 for (int k = 0; k <= kmax; ++k) o[k * T::SK + l] = r[k];
             }
         }

@@ -377,6 +377,12 @@ GRAD_STRAIGHT_MAX = 450
 # 17.1 -> 14.6, (dd|ps) 11.2 -> 9.2; but (ds|ps) (102 products) 10.0 -> 19.8
 # and (pp|ps) (124) 9.5 -> 13.3, which stay single-pass
 GRAD_SPLIT_MIN = 150
+# classes within GRAD_STRAIGHT_MAX that take the per-warp form all the same:
+# measured per class on (H2O)_32 6-31G* and (H2O)_16 def2-TZVP UHF against
+# the split per-lane form, e.g. (dp|ds) 16.3 -> 10.2 ms, (fs|pp) 45.6 ->
+# 19.4 ms, (fp|ps) 54.9 -> 38.3 ms (the per-lane form keeps (dp|ps), (ds|ds),
+# (fs|ps): 14.5 against 20.2, 5.6 against 9.2, 24.4 against 35.4 ms)
+GRAD_WARP = frozenset({'1111', '2011', '2120', '2210', '3011', '3020', '3110'})
 
 
 def grad_members(cls):
@@ -398,7 +404,7 @@ def gen_grad_struct(cls):
     li, lj, lk, ll = cls.li, cls.lj, cls.lk, cls.ll
     lines = []
     rects = grad_rects(cls)
-    small = len(grad_members(cls)) <= GRAD_STRAIGHT_MAX
+    small = len(grad_members(cls)) <= GRAD_STRAIGHT_MAX and cls.tag not in GRAD_WARP
     split = small and len(grad_members(cls)) > GRAD_SPLIT_MIN
     lines.append(f'    static constexpr bool G_SMALL = {"true" if small else "false"};')
     lines.append(f'    static constexpr bool G_SPLIT = {"true" if split else "false"};')

@@ -408,6 +408,7 @@ def gen_grad_struct(cls):
     split = small and len(grad_members(cls)) > GRAD_SPLIT_MIN
     lines.append(f'    static constexpr bool G_SMALL = {"true" if small else "false"};')
     lines.append(f'    static constexpr bool G_SPLIT = {"true" if split else "false"};')
+    lines.append(f'    static constexpr int G_NMEM = {len(grad_members(cls))};   // block products')
     for name, (e0, e1), (f0, f1), _ in rects:
         ne = len(_level_set(e0, e1))
         nf = len(_level_set(f0, f1))

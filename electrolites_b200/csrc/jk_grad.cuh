@@ -698,8 +698,19 @@ constexpr int grad_threads() { return C::G_SMALL ? 128 : 32 * GradTeam<C>::NW; }
 template <class C>
 constexpr size_t grad_team_doubles() { return C::G_SMALL ? 0 : (size_t)GradTeam<C>::SIZE; }
 
+// resident blocks per SM the per-lane kernels of the smallest classes
+// ((ss|ss), (ps|ss)) are compiled for: 4, at 128 registers (measured on
+// (H2O)_32 6-31G* UHF: (ps|ss) 10.6 -> 9.6 ms; (ps|ps) and (ds|ss) spill at
+// that cap and lose, 4.2 -> 7.6 and 3.9 -> 6.0 ms); the others take 255
+template <class C>
+constexpr int grad_min_blocks()
+{
+    return C::G_SMALL && !C::G_SPLIT && C::G_NMEM <= 20 ? 4 : 1;
+}
+
 template <class C, int NT>
-__global__ void __launch_bounds__(NT, 1) jk_grad_kernel(const __grid_constant__ LaunchParams<1> P)
+__global__ void __launch_bounds__(NT, grad_min_blocks<C>())
+    jk_grad_kernel(const __grid_constant__ LaunchParams<1> P)
 {
     const ClassArgs &A = P.a;
     constexpr int NW = NT / 32;

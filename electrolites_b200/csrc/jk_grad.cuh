@@ -698,14 +698,21 @@ constexpr int grad_threads() { return C::G_SMALL ? 128 : 32 * GradTeam<C>::NW; }
 template <class C>
 constexpr size_t grad_team_doubles() { return C::G_SMALL ? 0 : (size_t)GradTeam<C>::SIZE; }
 
-// resident blocks per SM the per-lane kernels of the smallest classes
-// ((ss|ss), (ps|ss)) are compiled for: 4, at 128 registers (measured on
-// (H2O)_32 6-31G* UHF: (ps|ss) 10.6 -> 9.6 ms; (ps|ps) and (ds|ss) spill at
-// that cap and lose, 4.2 -> 7.6 and 3.9 -> 6.0 ms); the others take 255
+// resident blocks per SM the gradient kernels are compiled for, measured
+// per class on (H2O)_32 6-31G* and (H2O)_16 def2-TZVP UHF: the per-lane
+// kernels of (ss|ss) and (ps|ss) at 4 (128 registers; (ps|ss) 10.6 -> 9.6
+// ms, while (ps|ps) and (ds|ss) spill at that cap and lose, 4.2 -> 7.6 and
+// 3.9 -> 6.0 ms), the other per-lane kernels at 1 (255 registers); the
+// per-warp kernels at 3 (at most 170 registers; shared memory allows 3:
+// (dp|ds) 10.2 -> 8.8 ms, (dd|ps) 8.3 -> 7.5, (dp|pp) 8.2 -> 7.6), except
+// (pp|pp), (dp|dp), (fp|ps), (fp|pp), which lose at 3 (7.2 -> 7.9, 6.8 ->
+// 8.2, 38.0 -> 43.7, 59.7 -> 70.5 ms) and keep 1
 template <class C>
 constexpr int grad_min_blocks()
 {
-    return C::G_SMALL && !C::G_SPLIT && C::G_NMEM <= 20 ? 4 : 1;
+    constexpr int tag = ((C::LI * 10 + C::LJ) * 10 + C::LK) * 10 + C::LL;
+    if constexpr (C::G_SMALL) return !C::G_SPLIT && C::G_NMEM <= 20 ? 4 : 1;
+    return tag == 1111 || tag == 2121 || tag == 3110 || tag == 3111 ? 1 : 3;
 }
 
 template <class C, int NT>

@@ -20,14 +20,19 @@
 // per block in shared memory (molecules of up to JK_GRAD_SMEM_ATOMS atoms)
 // and added to the output once per block and atom component: every quartet
 // adds to the same natm x 3 numbers, so global atomics per quartet would all
-// contend for a few hundred addresses.  Per quartet and
-// primitive quartet and Rys root, the code generator's grad_root adds the
-// root's 2D-integral products to four (e|f)-space blocks in registers: U
-// (unweighted), RA, RB, RC (weighted by 2 alpha of the primitive of shell i,
-// j, k); after the primitive sums the generated transfers of the shifted
-// shells give each derivative block, which is contracted with W on the fly.
-// The bra atoms' forces add up in registers over a task; the ket atoms'
-// go to memory per quartet.
+// contend for a few hundred addresses.  Two forms, chosen per class by
+// measurement in the code generator (G_SMALL):
+//   per lane: per quartet, primitive quartet and Rys root, the generated
+//   grad_root adds the root's 2D-integral products to four (e|f)-space
+//   blocks in registers: U (unweighted), RA, RB, RC (weighted by 2 alpha of
+//   the primitive of shell i, j, k); after the primitive sums the generated
+//   transfers of the shifted shells give each derivative block, which is
+//   contracted with W on the fly.  Classes with many block products
+//   (G_SPLIT) run one primitive pass per block so that one block is live at
+//   a time (four blocks spilled to local memory).  The bra atoms' forces add
+//   up in registers over a task; the ket atoms' go to the block's sums per
+//   quartet;
+//   per warp (the larger classes): see grad_team_quartet below.
 #pragma once
 
 // atoms whose forces a block sums in shared memory (24 KB) before adding
